@@ -1,0 +1,242 @@
+/*
+ * wwcuda.h -- C ABI of libwwcuda.so, the B200 (sm_100a) implementation of the
+ * WWocl search path: segmented wheel sieve + base-2 strong PRP test,
+ * Wieferich test 2^((p-1)/2) mod p^2 and Wall-Sun-Sun test F_{p-(p|5)} mod p^2,
+ * with the reference's checksum and hit records.
+ *
+ * It replaces the reference's device layer (simpleCL.h:63-140 / simpleCL.c)
+ * and its five OpenCL kernels.  Two levels:
+ *
+ *  1. Kernel-shaped entry points (ww_launch_*) that take the same arguments
+ *     as the reference kernels, as plain device pointers plus the buffer
+ *     capacities the reference left implicit and a cudaStream_t passed as
+ *     void*.  They allocate nothing and never synchronise.
+ *  2. A context (ww_ctx) that owns the stream, the device buffers and the
+ *     pinned read-back area -- the reference's progData (main.cpp:51-66)
+ *     plus its sclRead/sclFinish calls -- used by the wwocl host program.
+ *
+ * Conventions: every function returns an int status (WW_OK = 0, negative on
+ * error, see WW_ERR_*); ww_last_error() gives a message for the calling
+ * thread.  No function calls exit().  One host thread per ww_ctx.  All
+ * context calls are ordered on the context's stream.
+ */
+#ifndef WWCUDA_H
+#define WWCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WW_ABI_VERSION 1
+
+/* status codes */
+#define WW_OK 0
+#define WW_ERR_CUDA (-1)          /* a CUDA runtime call failed             */
+#define WW_ERR_ARG (-2)           /* bad argument (range, size, pointer)    */
+#define WW_ERR_PRP_OVERFLOW (-3)  /* PRP list longer than its buffer        */
+#define WW_ERR_HIT_OVERFLOW (-4)  /* more hits than the hit buffer holds    */
+#define WW_ERR_TIMEOUT (-5)       /* ww_sync gave up waiting                */
+#define WW_ERR_NOMEM (-6)         /* device or pinned allocation failed     */
+#define WW_ERR_COMPOSITE (-7)     /* a reported hit is composite            */
+#define WW_ERR_STATE (-8)         /* call out of order / no buffers         */
+#define WW_ERR_NODEV (-9)         /* no usable CUDA device                  */
+
+/* Hit record: the fields of gpuSpecialPrime / gpuResult / gpuRem / gpuQuot
+ * (main.cpp:52-56).  result 1093 = Wieferich, 1 = WSS prime, 2 = WSS
+ * special instance (wieferich.cl:248-293, wallsunsun.cl:325-349). */
+typedef struct {
+    uint64_t p;
+    int32_t result;
+    int32_t rem;
+    int32_t quot;
+    int32_t pad;
+} ww_hit;
+
+/* Device counters (main.cpp:1446-1493): checksum, result count, PRP count
+ * of the current launch (primecount[0]), largest launch PRP count
+ * (primecount[1]), PRPs tested since the last clear (totalprimecount). */
+typedef struct {
+    uint64_t checksum;
+    uint64_t total_prp_count;
+    uint32_t result_count;
+    uint32_t seg_prp_count;
+    uint32_t max_prp_count;
+    uint32_t overflow; /* bit 0: PRP list overflow, bit 1: hit overflow */
+} ww_counters;
+
+const char *ww_last_error(void);
+const char *ww_status_string(int status);
+int ww_abi_version(void);
+
+/* ---------------------------------------------------------------------------
+ * 1. Kernel-shaped entry points.  Device pointers; stream is a cudaStream_t
+ *    (NULL = legacy default stream).  Capacities bound every device write;
+ *    counters keep counting past them so the host can detect overflow.
+ * ------------------------------------------------------------------------- */
+
+/* clearn (clearn.cl:12-21): primecount[0] = 0. */
+int ww_launch_clearn(uint32_t *primecount, void *stream);
+
+/* clearresult (clearresult.cl:12-26): checksum, resultcount,
+ * totalprimecount and primecount[1] = 0. */
+int ww_launch_clearresult(uint64_t *checksum, uint32_t *resultcount, uint64_t *totalprimecount,
+                          uint32_t *primecount, void *stream);
+
+/* getsegprimes (getsegprimes.cl:228-301): every base-2 strong probable prime
+ * in [low, high) with no prime factor <= 113 is appended to g_prime, with
+ * q = p^-1 mod 2^64 in g_invert, counted in primecount[0].  low must be the
+ * wheel-aligned start and wheelidx its index from ww_find_wheel_offset
+ * (main.cpp:1716-1721); 127 <= low, high <= 2^64-1.  List order is
+ * unspecified.  *overflow |= 1 when more than capacity PRPs were found. */
+int ww_launch_getsegprimes(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime,
+                           uint64_t *g_invert, uint32_t *primecount, uint64_t capacity,
+                           uint32_t *overflow, void *stream);
+
+/* wieferich (wieferich.cl:196-328): for each of the primecount[0] PRPs,
+ * 2^((p-1)/2) mod p^2; hits appended to the SoA hit arrays (capacity
+ * numresults), checksum += high digit mod 2^32, totalprimecount +=
+ * primecount[0], primecount[1] = max(primecount[1], primecount[0]).
+ * g_invert and g_one may be NULL (computed in the kernel); when g_one is
+ * non-NULL the Montgomery one (2 words per PRP) is stored for wallsunsun. */
+int ww_launch_wieferich(uint32_t *primecount, const uint64_t *g_prime, const uint64_t *g_invert,
+                        uint64_t *g_one, uint64_t *special_prime, int32_t *rem, int32_t *quot,
+                        int32_t *result, uint64_t *checksum, uint32_t *resultcount,
+                        uint64_t *totalprimecount, uint64_t capacity, uint32_t numresults,
+                        uint32_t *overflow, void *stream);
+
+/* wallsunsun (wallsunsun.cl:221-354): F_{p-(p|5)} mod p^2 for each PRP;
+ * hits and checksum as above.  g_invert / g_one may be NULL. */
+int ww_launch_wallsunsun(const uint32_t *primecount, const uint64_t *g_prime,
+                         const uint64_t *g_invert, const uint64_t *g_one, uint64_t *special_prime,
+                         int32_t *rem, int32_t *quot, int32_t *result, uint64_t *checksum,
+                         uint32_t *resultcount, uint64_t capacity, uint32_t numresults,
+                         uint32_t *overflow, void *stream);
+
+/* Both tests in one kernel (no reference counterpart; replaces the
+ * wieferich + wallsunsun pair of main.cpp:1738-1741 with one launch).
+ * Same effect on checksum, hits and counters as the pair. */
+int ww_launch_test_prps(uint32_t *primecount, const uint64_t *g_prime, const uint64_t *g_invert,
+                        uint64_t *special_prime, int32_t *rem, int32_t *quot, int32_t *result,
+                        uint64_t *checksum, uint32_t *resultcount, uint64_t *totalprimecount,
+                        uint64_t capacity, uint32_t numresults, uint32_t *overflow, void *stream);
+
+/* Per-prime canonical digits for verification (no reference counterpart):
+ * out[4i..4i+3] = (s0, s1, c20, c21) with 2^((p-1)/2) = s0 + p s1 and
+ * F_{p-(p|5)} = c20 + p c21 mod p^2. */
+int ww_launch_digits(const uint64_t *primes, uint64_t n, uint64_t *out, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * 2. Context API (progData + simpleCL replacement).
+ * ------------------------------------------------------------------------- */
+
+typedef struct ww_ctx ww_ctx;
+
+/* Open device `device` (cudaSetDevice) and create the stream and counters. */
+int ww_open(int device, ww_ctx **out);
+void ww_close(ww_ctx *ctx);
+
+/* (Re)allocate the PRP buffers (prime, invert, one) for max_prps entries and
+ * the hit arrays for max_hits (numresults, main.cpp:1119). */
+int ww_reserve(ww_ctx *ctx, uint64_t max_prps, uint32_t max_hits);
+
+int ww_clear_results(ww_ctx *ctx); /* clearresult */
+int ww_clear_segment(ww_ctx *ctx); /* clearn */
+
+/* getsegprimes over [kernel_start, stop) into the context's PRP buffers. */
+int ww_sieve_prp(ww_ctx *ctx, uint64_t kernel_start, uint64_t stop, int32_t wheel_idx);
+int ww_wieferich(ww_ctx *ctx);
+int ww_wallsunsun(ww_ctx *ctx);
+int ww_test_prps(ww_ctx *ctx); /* fused wieferich + wallsunsun */
+
+/* Copy a host list of PRPs into the context's PRP buffer (sets the segment
+ * count, q computed on the device).  For fixed-list workloads. */
+int ww_load_prps(ww_ctx *ctx, const uint64_t *host_primes, uint64_t n);
+
+/* Record an event after the work queued so far; ww_wait_marker blocks until
+ * the event `slot` (0..7) completed or timeout_ms passed (the reference's
+ * launchEvent / waitOnEvent, main.cpp:329-377). */
+int ww_marker(ww_ctx *ctx, int slot);
+int ww_wait_marker(ww_ctx *ctx, int slot, uint32_t timeout_ms);
+
+/* Wait for all queued work (sclFinish / sleepCPU, main.cpp:381-446). */
+int ww_sync(ww_ctx *ctx, uint32_t timeout_ms);
+
+/* Blocking read-backs (sclRead of main.cpp:793-840). */
+int ww_read_counters(ww_ctx *ctx, ww_counters *out);
+int ww_read_hits(ww_ctx *ctx, ww_hit *out, uint32_t cap, uint32_t *n);
+int ww_read_prps(ww_ctx *ctx, uint64_t *out, uint64_t cap, uint64_t *n);
+
+/* Elapsed device milliseconds between two markers (ProfilesclEnqueueKernel,
+ * simpleCL.c:511-534). */
+int ww_marker_elapsed(ww_ctx *ctx, int slot_a, int slot_b, float *ms);
+
+/* Device pointers owned by the context (for the kernel-shaped calls). */
+typedef struct {
+    uint64_t *prime, *invert, *one;
+    uint64_t *special_prime;
+    int32_t *rem, *quot, *result;
+    uint64_t *checksum, *total_prp_count;
+    uint32_t *result_count, *primecount, *overflow;
+    uint64_t prp_capacity;
+    uint32_t hit_capacity;
+    void *stream;
+} ww_buffers;
+int ww_get_buffers(ww_ctx *ctx, ww_buffers *out);
+
+/* ---------------------------------------------------------------------------
+ * 3. Host helpers of the reference program (main.cpp), exported so every
+ *    caller shares one implementation.
+ * ------------------------------------------------------------------------- */
+
+/* findWheelOffset (main.cpp:528-587).  Returns WW_ERR_ARG when no number
+ * >= start below 2^64 is prime to 30. */
+int ww_find_wheel_offset(uint64_t *start, int32_t *index);
+
+/* isPrime (main.cpp:301-324) and isPRP (main.cpp:245-291), on the host. */
+int ww_is_prime(uint64_t n);
+int ww_is_prp(uint64_t n);
+
+/* START/END parsing (main.cpp:1193-1262): e-notation or decimal. */
+int ww_parse_number(const char *text, uint64_t *out);
+
+/* getResults formatting (main.cpp:843-916): sorts hits by p, writes the
+ * result lines of prime hits into buf, counts PRP-only hits in *dropped.
+ * Returns bytes written, WW_ERR_COMPOSITE for a composite hit, WW_ERR_ARG
+ * when buf is too small. */
+int ww_format_hits(ww_hit *hits, uint32_t n, char *buf, size_t cap, uint32_t *dropped);
+
+/* Upper bound on the number of base-2 strong PRPs in [lo, hi) used to size
+ * PRP buffers (replaces primesieve_count_primes, main.cpp:1087-1091). */
+uint64_t ww_prp_count_bound(uint64_t lo, uint64_t hi);
+
+/* Host twin of the kernels for the start-up self-test (testKernels,
+ * main.cpp:590-738): digits of a list (same layout as ww_launch_digits) and
+ * the PRP count, checksum and hit count of [lo, hi).  Never used to produce
+ * results, only to check the GPU against. */
+int ww_selftest_digits(const uint64_t *primes, uint64_t n, uint64_t *out);
+int ww_selftest_range(uint64_t lo, uint64_t hi, uint64_t *prp_count, uint64_t *checksum,
+                      uint32_t *result_count);
+
+/* ---------------------------------------------------------------------------
+ * 4. Measurement utilities (no reference counterpart).
+ * ------------------------------------------------------------------------- */
+
+/* First n numbers of the SplitMix64 stream for `seed` (each output forced
+ * odd, kept when >= 2^62) that pass deterministic Miller-Rabin, in stream
+ * order, into the host array out (the GPU runs the primality tests).
+ * *consumed receives the stream positions used.  Allocates its own scratch. */
+int ww_random_primes(int device, uint64_t seed, uint64_t n, uint64_t *out, uint64_t *consumed);
+
+/* Integer-pipe microbenchmark: mode 0 mad.lo.u32, 1 mad.hi.u32,
+ * 2 mad.wide.u32, 3 64x64->128 multiply (carry chain), 4 fma.rn.f64,
+ * 5 add.u32 chains.  Returns operations per second in *ops_per_s
+ * (one op = one PTX instruction of that kind per thread). */
+int ww_pipe_bench(int device, int mode, double *ops_per_s, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WWCUDA_H */

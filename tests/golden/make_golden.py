@@ -1,0 +1,153 @@
+"""Regenerate the golden fixtures in this folder from the reference's own CPU
+code (oracle/_ref/libwwref.so, compiled in place from the reference tree by
+oracle/Makefile).  Run from the repository root where the reference sources
+are mounted:
+
+    make -C oracle && python tests/golden/make_golden.py
+
+Outputs (small, committed):
+  ref_ranges.json  per-range PRP count, checksum and CPU result count
+  ref_terms.npz    per-prime low 32 bits of the Wieferich and WSS checksum
+                   terms and the wwcpu.cpp hit flags for fixed prime samples
+  ref_prps.json    PRP-list digests (count, sum, sha256 of the sorted list)
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+from oracle.oracle import Oracle, RefCPU  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+TOP = 2**64
+
+RANGES = [
+    ("small_3e6", 127, 3_000_000),
+    ("config1_5e7", 127, 50_000_000),
+    ("cross_2p32", 4_294_000_000, 4_295_500_000),
+    ("near_top_2e6", TOP - 2**35, TOP - 2**35 + 2_000_000),
+    ("top_1e8", 18446744073609551615, 18446744073709551615),
+    ("wieferich_special_window", 2276306935816523 - 1_000_000, 2276306935816523 + 1_000_000),
+    ("wss_special_window", 338772621946054253, 338772621946054253 + 2_000_000),
+    ("mid_2p48", 2**48, 2**48 + 3_000_000),
+]
+
+PRP_RANGES = [
+    ("prp_small", 127, 2_000_000),
+    ("prp_2p32", 2**32 - 1_000_000, 2**32 + 1_000_000),
+    ("prp_2p63", 2**63 - 500_000, 2**63 + 500_000),
+    ("prp_top", TOP - 1_000_001, TOP - 1),
+    ("prp_spsp", 1_373_653 - 100, 1_373_653 + 3_000_000),
+]
+
+
+def digest(arr: np.ndarray) -> dict:
+    arr = np.sort(np.asarray(arr, dtype=np.uint64))
+    return {
+        "count": int(arr.size),
+        "sum_mod_2_64": int(arr.sum(dtype=np.uint64)),
+        "sha256": hashlib.sha256(arr.astype("<u8").tobytes()).hexdigest(),
+    }
+
+
+def prime_samples(o: Oracle) -> dict[str, np.ndarray]:
+    rng = np.random.default_rng(20201226)
+    out = {}
+    out["small"] = np.array([p for p in range(127, 20000, 2) if o.is_prp(p)], dtype=np.uint64)
+    near32 = []
+    n = 2**32 - 20001
+    while len(near32) < 2000:
+        if o.is_prp(n):
+            near32.append(n)
+        n += 2
+    out["near_2p32"] = np.array(near32, dtype=np.uint64)
+    below32 = []
+    n = 2**32 - 1
+    while len(below32) < 500:
+        if o.is_prp(n):
+            below32.append(n)
+        n -= 2
+    out["below_2p32"] = np.array(below32, dtype=np.uint64)
+    top = []
+    n = TOP - 1
+    while len(top) < 2000:
+        if o.is_prp(n):
+            top.append(n)
+        n -= 2
+    out["near_2p64"] = np.array(top, dtype=np.uint64)
+    rnd = []
+    while len(rnd) < 4000:
+        c = int(rng.integers(0, 2**63, dtype=np.uint64)) * 2 + 1
+        if c > 113 and o.is_prp(c):
+            rnd.append(c)
+    out["random64"] = np.array(rnd, dtype=np.uint64)
+    spsp = [p for p in range(127, 3_000_000, 2) if o.is_prp(p) and not o.is_prime(p)]
+    out["spsp"] = np.array(spsp, dtype=np.uint64)
+    out["known_hits"] = np.array([2276306935816523, 338772621946054253], dtype=np.uint64)
+    return out
+
+
+def parse_tests_txt(path: Path) -> list[dict]:
+    """The reference's end-to-end vectors (tests.txt): 'START END', optional
+    hit lines, then the final 16-hex-digit checksum, blocks split by dashes."""
+    blocks, cur = [], []
+    for ln in path.read_text().splitlines():
+        ln = ln.strip()
+        if ln and set(ln) == {"-"}:
+            blocks.append(cur)
+            cur = []
+        elif ln and not ln.startswith("test cases"):
+            cur.append(ln)
+    blocks.append(cur)
+    cases = []
+    for lines in blocks:
+        if len(lines) < 2:
+            continue
+        start, end = lines[0].split()
+        cases.append({"start": start, "end": end, "hits": lines[1:-1], "checksum": lines[-1]})
+    return cases
+
+
+def main() -> None:
+    ref = RefCPU()
+    o = Oracle()
+    ref_tree = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    cases = parse_tests_txt(ref_tree / "tests.txt")
+    (OUT / "tests_txt.json").write_text(json.dumps(cases, indent=1) + "\n")
+    print(cases, flush=True)
+    ranges = {}
+    for name, lo, hi in RANGES:
+        r = ref.scan_range(lo, hi)
+        ranges[name] = {"lo": lo, "hi": hi, "prp_count": r["prp_count"],
+                        "checksum": "%016X" % r["checksum"], "cpu_results": r["cpu_results"]}
+        print(name, ranges[name], flush=True)
+    (OUT / "ref_ranges.json").write_text(json.dumps(ranges, indent=1) + "\n")
+
+    prps = {}
+    for name, lo, hi in PRP_RANGES:
+        lst = ref.prp_list(lo, hi, cap=(hi - lo) // 2 + 16)
+        prps[name] = {"lo": lo, "hi": hi, **digest(lst)}
+        print(name, prps[name], flush=True)
+    (OUT / "ref_prps.json").write_text(json.dumps(prps, indent=1) + "\n")
+
+    samples = prime_samples(o)
+    arrays = {}
+    for name, ps in samples.items():
+        wt, st, wh, sh = ref.list_terms(ps)
+        arrays[f"{name}_p"] = ps
+        arrays[f"{name}_wterm"] = wt
+        arrays[f"{name}_sterm"] = st
+        arrays[f"{name}_whit"] = wh.astype(np.int8)
+        arrays[f"{name}_shit"] = sh.astype(np.int8)
+        print(name, ps.size, flush=True)
+    np.savez_compressed(OUT / "ref_terms.npz", **arrays)
+
+
+if __name__ == "__main__":
+    main()

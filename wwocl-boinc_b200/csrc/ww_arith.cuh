@@ -1,0 +1,341 @@
+// ww_arith.cuh -- exact modular arithmetic for the WWocl search path.
+//
+// Compiles for the device (sm_100a) and for the host, so the same algorithm
+// runs in the GPU kernels and in the host self-test.
+//
+//  mod n   : Montgomery, R = 2^64, with q = n^-1 mod 2^64 (the value the
+//            reference's getsegprimes stores in g_invert, getsegprimes.cl:70-75)
+//  mod p^2 : residues X = x0 + p*x1 (0 <= x0, x1 < p) in Montgomery form with
+//            R = 2^64, the "two-digit" representation of Dorais and Klyve
+//            (J. Integer Sequences 14, 2011) that the reference kernels use
+//            (wieferich.cl:111-193).  Products reduce the low digit by one
+//            REDC modulo p and the carry digit by a second one.
+//
+// The 64x64 products come from `mul_wide`/`mul_hi` (__umul64hi on the
+// device, which lowers to 32-bit multiply-adds on the integer pipe).
+#pragma once
+
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define WW_HD __host__ __device__ __forceinline__
+#else
+#define WW_HD inline
+#endif
+
+namespace ww {
+
+typedef unsigned long long u64;
+typedef unsigned int u32;
+
+struct D2 {
+    u64 d0, d1;  // value = d0 + p * d1
+};
+
+// ------------------------------------------------------------ 64-bit products
+
+WW_HD u64 mul_hi(u64 a, u64 b) {
+#if defined(__CUDA_ARCH__)
+    return __umul64hi(a, b);
+#else
+    return (u64)(((unsigned __int128)a * b) >> 64);
+#endif
+}
+
+WW_HD void mul_wide(u64 a, u64 b, u64 &lo, u64 &hi) {
+    lo = a * b;
+    hi = mul_hi(a, b);
+}
+
+// n^-1 mod 2^64 (Newton; n*n = 1 mod 8 seeds 3 correct bits).
+WW_HD u64 inv64(u64 n) {
+    u64 x = n;
+    x *= 2 - n * x;
+    x *= 2 - n * x;
+    x *= 2 - n * x;
+    x *= 2 - n * x;
+    x *= 2 - n * x;
+    return x;
+}
+
+// ------------------------------------------------------------------- mod n
+
+WW_HD u64 add_mod(u64 a, u64 b, u64 n) {  // a <= n, b < n
+    u64 s = a + b;
+    return (s < a || s >= n) ? s - n : s;
+}
+
+WW_HD u64 sub_mod(u64 a, u64 b, u64 n) {  // a < n, b <= n
+    return a >= b ? a - b : a - b + n;
+}
+
+// (hi:lo) * 2^-64 mod n for (hi:lo) < n * 2^64, q = n^-1 mod 2^64.
+WW_HD u64 redc(u64 lo, u64 hi, u64 n, u64 q) {
+    u64 u = lo * q;
+    u64 v = mul_hi(u, n);
+    return hi >= v ? hi - v : hi - v + n;
+}
+
+WW_HD u64 mont_mul(u64 a, u64 b, u64 n, u64 q) {
+    u64 lo, hi;
+    mul_wide(a, b, lo, hi);
+    return redc(lo, hi, n, q);
+}
+
+// 2^64 mod n for odd n > 1.
+WW_HD u64 r_mod(u64 n) {
+    if (n >> 63) return 0 - n;  // 2^64 - n < n
+    return (0 - n) % n;
+}
+
+// Base-2 strong probable-prime test (prime.h:65-114, getsegprimes.cl:118-164)
+// written as one uniform loop over the bits of n-1 so that a warp's lanes
+// stay converged whatever the 2-adic valuation t of n-1 is: the trailing t
+// zero bits square without doubling, and the checks fire at bit t (a^d = +-1)
+// and below it (a^(d 2^s) = -1).  Returns the result and n^-1 mod 2^64.
+WW_HD bool sprp2(u64 n, u64 &q_out) {
+    const u64 q = inv64(n);
+    q_out = q;
+    const u64 one = r_mod(n);
+    const u64 mone = n - one;
+    const u64 nm1 = n - 1;
+#if defined(__CUDA_ARCH__)
+    const int t = __ffsll((long long)nm1) - 1;
+    const int top = 63 - __clzll((long long)nm1);
+#else
+    const int t = __builtin_ctzll(nm1);
+    const int top = 63 - __builtin_clzll(nm1);
+#endif
+    u64 a = add_mod(one, one, n);  // 2 for the leading bit
+    bool ok = false;
+    for (int i = top - 1; i >= 1; --i) {
+        a = mont_mul(a, a, n, q);
+        const u64 d = add_mod(a, a, n);
+        a = ((nm1 >> i) & 1) ? d : a;
+        ok |= (i == t) & ((a == one) | (a == mone));
+        ok |= (i < t) & (a == mone);
+    }
+    if (t == 0) ok = false;  // even n is never a candidate
+    // t == top (n-1 a power of two) never happens for the odd n >= 127 tested
+    return ok;
+}
+
+// ----------------------------------------------------------------- mod p^2
+
+struct ModP2 {
+    u64 p, q;  // q = p^-1 mod 2^64
+};
+
+WW_HD D2 m2_add(D2 x, D2 y, u64 p) {
+    D2 r;
+    u64 s = x.d0 + y.d0;
+    bool c = (s < x.d0) | (s >= p);
+    r.d0 = c ? s - p : s;
+    u64 h = x.d1 + (u64)c;  // <= p
+    u64 t = h + y.d1;
+    r.d1 = ((t < h) | (t >= p)) ? t - p : t;
+    return r;
+}
+
+WW_HD D2 m2_sub(D2 x, D2 y, u64 p) {
+    D2 r;
+    bool b = x.d0 < y.d0;
+    r.d0 = b ? x.d0 - y.d0 + p : x.d0 - y.d0;
+    u64 t = y.d1 + (u64)b;  // <= p
+    r.d1 = x.d1 >= t ? x.d1 - t : x.d1 - t + p;
+    return r;
+}
+
+WW_HD D2 m2_dbl(D2 x, u64 p) { return m2_add(x, x, p); }
+
+// Finish a product: A = (alo, ahi) is x0*y0, (clo, chi, ctop) the cross sum
+// x0*y1 + x1*y0 (129 bits).  Montgomery: X*Y*2^-64 = (A - u p)/2^64
+// + p * ((C + u) * 2^-64 mod p), u = alo * q.
+WW_HD D2 m2_finish(u64 alo, u64 ahi, u64 clo, u64 chi, u64 ctop, u64 p, u64 q) {
+    const u64 u = alo * q;
+    const u64 v = mul_hi(u, p);
+    D2 r;
+    const bool b = ahi < v;
+    r.d0 = b ? ahi - v + p : ahi - v;
+    // C + u
+    u64 s = clo + u;
+    u64 c = s < clo;
+    u64 h = chi + c;
+    ctop += (h < c);
+    // high part < 2p: reduce once
+    if (ctop | (h >= p)) h -= p;
+    const u64 u2 = s * q;
+    const u64 v2 = mul_hi(u2, p);
+    const u64 t = v2 + (u64)b;  // <= p
+    r.d1 = h >= t ? h - t : h - t + p;
+    return r;
+}
+
+WW_HD D2 m2_mul(D2 x, D2 y, u64 p, u64 q) {
+    u64 alo, ahi, l1, h1, l2, h2;
+    mul_wide(x.d0, y.d0, alo, ahi);
+    mul_wide(x.d0, y.d1, l1, h1);
+    mul_wide(x.d1, y.d0, l2, h2);
+    u64 clo = l1 + l2;
+    u64 c = clo < l1;
+    u64 chi = h1 + h2;
+    u64 ctop = chi < h1;
+    chi += c;
+    ctop += chi < c;
+    return m2_finish(alo, ahi, clo, chi, ctop, p, q);
+}
+
+WW_HD D2 m2_sqr(D2 x, u64 p, u64 q) {
+    u64 alo, ahi, l, h;
+    mul_wide(x.d0, x.d0, alo, ahi);
+    mul_wide(x.d0, x.d1, l, h);
+    const u64 ctop = h >> 63;
+    const u64 chi = (h << 1) | (l >> 63);
+    const u64 clo = l << 1;
+    return m2_finish(alo, ahi, clo, chi, ctop, p, q);
+}
+
+// Leave Montgomery form: canonical digits of X * 2^-64 mod p^2.
+WW_HD D2 m2_redc(D2 x, u64 p, u64 q) { return m2_finish(x.d0, 0, x.d1, 0, 0, p, q); }
+
+// 2^64 mod p^2 as digits: the Montgomery form of 1 (wieferich.cl:116-126).
+WW_HD D2 m2_one(u64 p) {
+    D2 r;
+    if ((p >> 32) == 0) {
+        const u64 p2 = p * p;
+        const u64 rr = (0 - p2) % p2;
+        r.d0 = rr % p;
+        r.d1 = rr / p;
+        return r;
+    }
+    if (p >> 63) {  // 2^64 = (2^64 - p) + 1 * p
+        r.d0 = 0 - p;
+        r.d1 = 1;
+        return r;
+    }
+    const u64 mp = 0 - p;
+    r.d0 = mp % p;
+    r.d1 = mp / p + 1;
+    return r;
+}
+
+// x / 5 mod p for 0 <= x < p, p prime to 5; also returns j with 5y = x + j p.
+WW_HD u64 div5_mod(u64 x, u64 p, u32 pm5, u32 &j) {
+    // inverse of p mod 5 for residues 1..4: 1, 3, 2, 4
+    const u32 inv = (0x42310u >> (4 * pm5)) & 0xF;  // nibbles 0..4: 0, 1, 3, 2, 4
+    const u32 xm5 = (u32)(x % 5);
+    j = ((5 - xm5) * inv) % 5;
+    return (x + (u64)j * p) * 0xCCCCCCCCCCCCCCCDull;  // exact division by 5 mod 2^64
+}
+
+// Canonical digits t -> digits of t / 5 mod p^2.
+WW_HD D2 m2_div5(D2 t, u64 p) {
+    const u32 pm5 = (u32)(p % 5);
+    u32 j0, j1;
+    D2 y;
+    y.d0 = div5_mod(t.d0, p, pm5, j0);
+    y.d1 = div5_mod(sub_mod(t.d1, (u64)j0, p), p, pm5, j1);
+    return y;
+}
+
+// ------------------------------------------------------------ the two tests
+
+// 2^((p-1)/2) mod p^2 as canonical digits (wieferich.cl:219-245).
+WW_HD D2 wieferich_digits(u64 p, u64 q, D2 one) {
+    const u64 e = p >> 1;
+#if defined(__CUDA_ARCH__)
+    const int top = 63 - __clzll((long long)e);
+#else
+    const int top = 63 - __builtin_clzll(e);
+#endif
+    D2 a = m2_dbl(one, p);
+    for (int i = top - 1; i >= 0; --i) {
+        a = m2_sqr(a, p, q);
+        const D2 d = m2_dbl(a, p);
+        const bool bit = (e >> i) & 1;
+        a.d0 = bit ? d.d0 : a.d0;
+        a.d1 = bit ? d.d1 : a.d1;
+    }
+    return m2_redc(a, p, q);
+}
+
+// F_{p-(p|5)} mod p^2 as canonical digits.  The reference walks the
+// (F_k, F_{k-1}) doubling ladder, two squarings and a product per bit
+// (wallsunsun.cl:242-300).  Here the Lucas numbers V_k = L_k run a
+// Montgomery ladder (V_k, V_{k+1}), one squaring and one product per bit:
+//   V_2k = V_k^2 - 2(-1)^k,  V_2k+1 = V_k V_k+1 - (-1)^k,
+//   V_2k+2 = V_k+1^2 + 2(-1)^k,
+// and F_n = (2 V_{n+1} - V_n) / 5 gives the same residue exactly.
+WW_HD D2 wss_digits(u64 p, u64 q, D2 one) {
+    const u32 pm5 = (u32)(p % 5);
+    const u64 n = (pm5 == 2 || pm5 == 3) ? p + 1 : p - 1;  // p - (p|5)
+#if defined(__CUDA_ARCH__)
+    const int top = 63 - __clzll((long long)n);
+#else
+    const int top = 63 - __builtin_clzll(n);
+#endif
+    const D2 zero = {0, 0};
+    const D2 two = m2_dbl(one, p);
+    const D2 mone = m2_sub(zero, one, p);
+    const D2 mtwo = m2_sub(zero, two, p);
+    D2 A = one;                 // V_1
+    D2 B = m2_add(two, one, p); // V_2
+    bool odd = true;            // parity of the ladder index k
+    for (int i = top - 1; i >= 0; --i) {
+        const bool bit = (n >> i) & 1;
+        D2 s;
+        s.d0 = bit ? B.d0 : A.d0;
+        s.d1 = bit ? B.d1 : A.d1;
+        const D2 sq = m2_sqr(s, p, q);
+        const D2 pr = m2_mul(A, B, p, q);
+        // pr - (-1)^k ; sq -/+ 2(-1)^k
+        D2 cp, cs;
+        cp.d0 = odd ? one.d0 : mone.d0;
+        cp.d1 = odd ? one.d1 : mone.d1;
+        const bool plus2 = bit ^ odd;  // bit=0: -2(-1)^k, bit=1: +2(-1)^k
+        cs.d0 = plus2 ? two.d0 : mtwo.d0;
+        cs.d1 = plus2 ? two.d1 : mtwo.d1;
+        const D2 np = m2_add(pr, cp, p);
+        const D2 ns = m2_add(sq, cs, p);
+        A.d0 = bit ? np.d0 : ns.d0;
+        A.d1 = bit ? np.d1 : ns.d1;
+        B.d0 = bit ? ns.d0 : np.d0;
+        B.d1 = bit ? ns.d1 : np.d1;
+        odd = bit;
+    }
+    const D2 t = m2_redc(m2_sub(m2_dbl(B, p), A, p), p, q);
+    return m2_div5(t, p);
+}
+
+// ------------------------------------------------------------ classification
+
+constexpr u64 kThreshold = 1000;  // WW.h:8 SPECIAL_THRESHOLD
+
+// wieferich.cl:248-293.  Returns true and fills rem/quot for a hit.
+WW_HD bool wieferich_classify(u64 p, D2 s, int &rem, int &quot) {
+    if (((s.d1 == 0) & (s.d0 == 1)) | ((s.d1 == p - 1) & (s.d0 == p - 1))) {
+        rem = 1;
+        quot = 0;
+        return true;
+    }
+    if (s.d1 <= kThreshold) {
+        if (s.d0 == 1) { rem = 1; quot = (int)s.d1; return true; }
+        if (s.d0 == p - 1) { rem = -1; quot = (int)(s.d1 + 1); return true; }
+        return false;
+    }
+    if (s.d1 >= p - kThreshold) {
+        if (s.d0 == 1) { rem = 1; quot = (int)(s.d1 - p); return true; }
+        if (s.d0 == p - 1) { rem = -1; quot = (int)(s.d1 + 1 - p); return true; }
+    }
+    return false;
+}
+
+// wallsunsun.cl:325-349.  result 1 = WSS prime, 2 = special instance.
+WW_HD bool wss_classify(u64 p, D2 c, int &result, int &quot) {
+    if (c.d1 == 0) { result = 1; quot = 0; return true; }
+    if (c.d1 <= kThreshold) { result = 2; quot = (int)c.d1; return true; }
+    if (c.d1 >= p - kThreshold) { result = 2; quot = (int)(c.d1 - p); return true; }
+    return false;
+}
+
+}  // namespace ww

@@ -1,0 +1,504 @@
+// ww_capi.cu -- the C ABI of libwwcuda.so (include/wwcuda.h): kernel-shaped
+// launchers and the ww_ctx context that replaces the reference's progData +
+// simpleCL layer (main.cpp:51-90, simpleCL.c:352-719).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <thread>
+
+#include "../../include/wwcuda.h"
+#include "ww_kernels.cuh"
+
+using namespace ww;
+
+namespace {
+thread_local char g_err[512] = "";
+}  // namespace
+
+namespace ww {
+// Message for ww_last_error(), per calling thread (shared with ww_host.cpp).
+void set_err(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+}  // namespace ww
+
+namespace {
+
+#define WW_CU(call)                                                                        \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            set_err("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return WW_ERR_CUDA;                                                            \
+        }                                                                                  \
+    } while (0)
+
+#define WW_CHECK_LAUNCH() WW_CU(cudaGetLastError())
+
+int sm_count() {
+    int dev = 0, n = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int wheel_index_of(uint64_t n) {
+    switch (n % 30) {
+        case 7: return 0;
+        case 11: return 1;
+        case 13: return 2;
+        case 17: return 3;
+        case 19: return 4;
+        case 23: return 5;
+        case 29: return 6;
+        case 1: return 7;
+        default: return -1;
+    }
+}
+
+int test_grid() { return sm_count() * 4; }
+
+}  // namespace
+
+extern "C" {
+
+const char *ww_last_error(void) { return g_err; }
+
+const char *ww_status_string(int s) {
+    switch (s) {
+        case WW_OK: return "ok";
+        case WW_ERR_CUDA: return "CUDA error";
+        case WW_ERR_ARG: return "bad argument";
+        case WW_ERR_PRP_OVERFLOW: return "PRP buffer overflow";
+        case WW_ERR_HIT_OVERFLOW: return "hit buffer overflow";
+        case WW_ERR_TIMEOUT: return "timeout";
+        case WW_ERR_NOMEM: return "out of memory";
+        case WW_ERR_COMPOSITE: return "composite hit";
+        case WW_ERR_STATE: return "bad state";
+        case WW_ERR_NODEV: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+int ww_abi_version(void) { return WW_ABI_VERSION; }
+
+// ------------------------------------------------------------------ launchers
+
+int ww_launch_clearn(uint32_t *primecount, void *stream) {
+    if (!primecount) return set_err("null primecount"), WW_ERR_ARG;
+    WW_CU(cudaMemsetAsync(primecount, 0, sizeof(uint32_t), as_stream(stream)));
+    return WW_OK;
+}
+
+int ww_launch_clearresult(uint64_t *checksum, uint32_t *resultcount, uint64_t *totalprimecount,
+                          uint32_t *primecount, void *stream) {
+    if (!checksum || !resultcount || !totalprimecount || !primecount)
+        return set_err("null counter pointer"), WW_ERR_ARG;
+    cudaStream_t s = as_stream(stream);
+    WW_CU(cudaMemsetAsync(checksum, 0, sizeof(uint64_t), s));
+    WW_CU(cudaMemsetAsync(resultcount, 0, sizeof(uint32_t), s));
+    WW_CU(cudaMemsetAsync(totalprimecount, 0, sizeof(uint64_t), s));
+    WW_CU(cudaMemsetAsync(primecount + 1, 0, sizeof(uint32_t), s));
+    return WW_OK;
+}
+
+int ww_launch_getsegprimes(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime,
+                           uint64_t *g_invert, uint32_t *primecount, uint64_t capacity,
+                           uint32_t *overflow, void *stream) {
+    if (!g_prime || !g_invert || !primecount || !overflow) return set_err("null pointer"), WW_ERR_ARG;
+    if (low < 127 || high <= low) return set_err("bad range [%llu, %llu)", (unsigned long long)low,
+                                                  (unsigned long long)high), WW_ERR_ARG;
+    if (wheel_index_of(low) != wheelidx)
+        return set_err("wheel index %d does not match start %llu", wheelidx, (unsigned long long)low),
+               WW_ERR_ARG;
+    if (ww_prp_count_bound(low, high) >= 0xffffffffull)
+        return set_err("range too wide for a 32-bit PRP counter"), WW_ERR_ARG;
+    const uint64_t b0 = low & ~1ull;
+    const uint64_t span = high - b0;
+    const uint64_t per = 2ull * kSegOdd;
+    const uint64_t nseg = span / per + (span % per ? 1 : 0);
+    const uint64_t grid = nseg < (uint64_t)sm_count() * 6 ? nseg : (uint64_t)sm_count() * 6;
+    PrpOut out{(u64 *)g_prime, (u64 *)g_invert, primecount, capacity, overflow};
+    k_sieve_prp<<<(unsigned)grid, kSieveThreads, 0, as_stream(stream)>>>(low, high, nseg, out);
+    WW_CHECK_LAUNCH();
+    return WW_OK;
+}
+
+int ww_launch_wieferich(uint32_t *primecount, const uint64_t *g_prime, const uint64_t *g_invert,
+                        uint64_t *g_one, uint64_t *special_prime, int32_t *rem, int32_t *quot,
+                        int32_t *result, uint64_t *checksum, uint32_t *resultcount,
+                        uint64_t *totalprimecount, uint64_t capacity, uint32_t numresults,
+                        uint32_t *overflow, void *stream) {
+    if (!primecount || !g_prime || !special_prime || !rem || !quot || !result || !checksum ||
+        !resultcount || !totalprimecount || !overflow)
+        return set_err("null pointer"), WW_ERR_ARG;
+    HitOut h{(u64 *)special_prime, rem, quot, result, resultcount, numresults, overflow};
+    k_wieferich<<<test_grid(), kTestThreads, 0, as_stream(stream)>>>(
+        primecount, (const u64 *)g_prime, (const u64 *)g_invert, (u64 *)g_one, h, (u64 *)checksum,
+        (u64 *)totalprimecount, capacity);
+    WW_CHECK_LAUNCH();
+    return WW_OK;
+}
+
+int ww_launch_wallsunsun(const uint32_t *primecount, const uint64_t *g_prime,
+                         const uint64_t *g_invert, const uint64_t *g_one, uint64_t *special_prime,
+                         int32_t *rem, int32_t *quot, int32_t *result, uint64_t *checksum,
+                         uint32_t *resultcount, uint64_t capacity, uint32_t numresults,
+                         uint32_t *overflow, void *stream) {
+    if (!primecount || !g_prime || !special_prime || !rem || !quot || !result || !checksum ||
+        !resultcount || !overflow)
+        return set_err("null pointer"), WW_ERR_ARG;
+    HitOut h{(u64 *)special_prime, rem, quot, result, resultcount, numresults, overflow};
+    k_wallsunsun<<<test_grid(), kTestThreads, 0, as_stream(stream)>>>(
+        primecount, (const u64 *)g_prime, (const u64 *)g_invert, (const u64 *)g_one, h,
+        (u64 *)checksum, capacity);
+    WW_CHECK_LAUNCH();
+    return WW_OK;
+}
+
+int ww_launch_test_prps(uint32_t *primecount, const uint64_t *g_prime, const uint64_t *g_invert,
+                        uint64_t *special_prime, int32_t *rem, int32_t *quot, int32_t *result,
+                        uint64_t *checksum, uint32_t *resultcount, uint64_t *totalprimecount,
+                        uint64_t capacity, uint32_t numresults, uint32_t *overflow, void *stream) {
+    if (!primecount || !g_prime || !special_prime || !rem || !quot || !result || !checksum ||
+        !resultcount || !totalprimecount || !overflow)
+        return set_err("null pointer"), WW_ERR_ARG;
+    HitOut h{(u64 *)special_prime, rem, quot, result, resultcount, numresults, overflow};
+    k_test_prps<<<test_grid(), kTestThreads, 0, as_stream(stream)>>>(
+        primecount, (const u64 *)g_prime, (const u64 *)g_invert, h, (u64 *)checksum,
+        (u64 *)totalprimecount, capacity);
+    WW_CHECK_LAUNCH();
+    return WW_OK;
+}
+
+int ww_launch_digits(const uint64_t *primes, uint64_t n, uint64_t *out, void *stream) {
+    if (!primes || !out) return set_err("null pointer"), WW_ERR_ARG;
+    if (n == 0) return WW_OK;
+    uint64_t blocks = (n + kTestThreads - 1) / kTestThreads;
+    if (blocks > (uint64_t)test_grid() * 8) blocks = (uint64_t)test_grid() * 8;
+    k_digits<<<(unsigned)blocks, kTestThreads, 0, as_stream(stream)>>>((const u64 *)primes, n, (u64 *)out);
+    WW_CHECK_LAUNCH();
+    return WW_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ context
+
+namespace {
+
+struct DevCounters {
+    unsigned long long checksum;
+    unsigned long long total;
+    unsigned int resultcount;
+    unsigned int primecount[2];
+    unsigned int overflow;
+};
+
+__global__ void k_set_count(unsigned int *pc, unsigned int v) { pc[0] = v; }
+
+}  // namespace
+
+struct ww_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    DevCounters *dc = nullptr;
+    DevCounters *hc = nullptr;  // pinned
+    u64 *prime = nullptr, *inv = nullptr, *one = nullptr;
+    u64 cap = 0;
+    u64 *hprime = nullptr;
+    int *hrem = nullptr, *hquot = nullptr, *hres = nullptr;
+    u32 hcap = 0;
+    cudaEvent_t ev[8] = {};
+};
+
+extern "C" {
+
+int ww_open(int device, ww_ctx **out) {
+    if (!out) return set_err("null out"), WW_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0)
+        return set_err("no CUDA device %d (count %d)", device, ndev), WW_ERR_NODEV;
+    WW_CU(cudaSetDevice(device));
+    ww_ctx *c = new (std::nothrow) ww_ctx;
+    if (!c) return set_err("host allocation failed"), WW_ERR_NOMEM;
+    c->device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->dc, sizeof(DevCounters));
+    if (e == cudaSuccess) e = cudaMallocHost(&c->hc, sizeof(DevCounters));
+    for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->dc, 0, sizeof(DevCounters), c->stream);
+    if (e != cudaSuccess) {
+        set_err("ww_open: %s", cudaGetErrorString(e));
+        ww_close(c);
+        return WW_ERR_CUDA;
+    }
+    *out = c;
+    return WW_OK;
+}
+
+void ww_close(ww_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaFree(c->prime);
+    cudaFree(c->inv);
+    cudaFree(c->one);
+    cudaFree(c->hprime);
+    cudaFree(c->hrem);
+    cudaFree(c->hquot);
+    cudaFree(c->hres);
+    cudaFree(c->dc);
+    if (c->hc) cudaFreeHost(c->hc);
+    for (int i = 0; i < 8; ++i)
+        if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int ww_reserve(ww_ctx *c, uint64_t max_prps, uint32_t max_hits) {
+    if (!c || max_prps == 0 || max_hits == 0) return set_err("bad reserve arguments"), WW_ERR_ARG;
+    WW_CU(cudaSetDevice(c->device));
+    WW_CU(cudaStreamSynchronize(c->stream));
+    if (max_prps != c->cap) {
+        cudaFree(c->prime);
+        cudaFree(c->inv);
+        cudaFree(c->one);
+        c->prime = c->inv = c->one = nullptr;
+        c->cap = 0;
+        if (cudaMalloc(&c->prime, max_prps * 8) != cudaSuccess ||
+            cudaMalloc(&c->inv, max_prps * 8) != cudaSuccess ||
+            cudaMalloc(&c->one, max_prps * 16) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(c->prime);
+            cudaFree(c->inv);
+            cudaFree(c->one);
+            c->prime = c->inv = c->one = nullptr;
+            return set_err("cannot allocate PRP buffers for %llu entries", (unsigned long long)max_prps),
+                   WW_ERR_NOMEM;
+        }
+        c->cap = max_prps;
+    }
+    if (max_hits != c->hcap) {
+        cudaFree(c->hprime);
+        cudaFree(c->hrem);
+        cudaFree(c->hquot);
+        cudaFree(c->hres);
+        c->hprime = nullptr;
+        c->hrem = c->hquot = c->hres = nullptr;
+        c->hcap = 0;
+        if (cudaMalloc(&c->hprime, (size_t)max_hits * 8) != cudaSuccess ||
+            cudaMalloc(&c->hrem, (size_t)max_hits * 4) != cudaSuccess ||
+            cudaMalloc(&c->hquot, (size_t)max_hits * 4) != cudaSuccess ||
+            cudaMalloc(&c->hres, (size_t)max_hits * 4) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err("cannot allocate hit buffers"), WW_ERR_NOMEM;
+        }
+        c->hcap = max_hits;
+    }
+    return WW_OK;
+}
+
+int ww_get_buffers(ww_ctx *c, ww_buffers *b) {
+    if (!c || !b) return set_err("null argument"), WW_ERR_ARG;
+    b->prime = (uint64_t *)c->prime;
+    b->invert = (uint64_t *)c->inv;
+    b->one = (uint64_t *)c->one;
+    b->special_prime = (uint64_t *)c->hprime;
+    b->rem = c->hrem;
+    b->quot = c->hquot;
+    b->result = c->hres;
+    b->checksum = (uint64_t *)&c->dc->checksum;
+    b->total_prp_count = (uint64_t *)&c->dc->total;
+    b->result_count = &c->dc->resultcount;
+    b->primecount = c->dc->primecount;
+    b->overflow = &c->dc->overflow;
+    b->prp_capacity = c->cap;
+    b->hit_capacity = c->hcap;
+    b->stream = c->stream;
+    return WW_OK;
+}
+
+int ww_clear_results(ww_ctx *c) {
+    if (!c) return set_err("null ctx"), WW_ERR_ARG;
+    int rc = ww_launch_clearresult((uint64_t *)&c->dc->checksum, &c->dc->resultcount, (uint64_t *)&c->dc->total,
+                                   c->dc->primecount, c->stream);
+    if (rc) return rc;
+    WW_CU(cudaMemsetAsync(&c->dc->overflow, 0, sizeof(unsigned int), c->stream));
+    return WW_OK;
+}
+
+int ww_clear_segment(ww_ctx *c) {
+    if (!c) return set_err("null ctx"), WW_ERR_ARG;
+    return ww_launch_clearn(c->dc->primecount, c->stream);
+}
+
+#define WW_NEED_BUFFERS(c)                                                        \
+    do {                                                                          \
+        if (!(c)) return set_err("null ctx"), WW_ERR_ARG;                         \
+        if (!(c)->prime || !(c)->hprime) return set_err("ww_reserve first"), WW_ERR_STATE; \
+    } while (0)
+
+int ww_sieve_prp(ww_ctx *c, uint64_t kernel_start, uint64_t stop, int32_t wheel_idx) {
+    WW_NEED_BUFFERS(c);
+    return ww_launch_getsegprimes(kernel_start, stop, wheel_idx, (uint64_t *)c->prime, (uint64_t *)c->inv, c->dc->primecount,
+                                  c->cap, &c->dc->overflow, c->stream);
+}
+
+int ww_wieferich(ww_ctx *c) {
+    WW_NEED_BUFFERS(c);
+    return ww_launch_wieferich(c->dc->primecount, (uint64_t *)c->prime, (uint64_t *)c->inv, (uint64_t *)c->one,
+                               (uint64_t *)c->hprime, c->hrem, c->hquot, c->hres, (uint64_t *)&c->dc->checksum,
+                               &c->dc->resultcount, (uint64_t *)&c->dc->total, c->cap,
+                               c->hcap, &c->dc->overflow, c->stream);
+}
+
+int ww_wallsunsun(ww_ctx *c) {
+    WW_NEED_BUFFERS(c);
+    return ww_launch_wallsunsun(c->dc->primecount, (uint64_t *)c->prime, (uint64_t *)c->inv, (uint64_t *)c->one,
+                                (uint64_t *)c->hprime, c->hrem, c->hquot, c->hres, (uint64_t *)&c->dc->checksum,
+                                &c->dc->resultcount, c->cap, c->hcap,
+                                &c->dc->overflow, c->stream);
+}
+
+int ww_test_prps(ww_ctx *c) {
+    WW_NEED_BUFFERS(c);
+    return ww_launch_test_prps(c->dc->primecount, (uint64_t *)c->prime, (uint64_t *)c->inv, (uint64_t *)c->hprime,
+                               c->hrem, c->hquot, c->hres, (uint64_t *)&c->dc->checksum, &c->dc->resultcount,
+                               (uint64_t *)&c->dc->total, c->cap, c->hcap,
+                               &c->dc->overflow, c->stream);
+}
+
+int ww_load_prps(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
+    WW_NEED_BUFFERS(c);
+    if (n > c->cap || n > 0xffffffffull || (!host_primes && n))
+        return set_err("list of %llu PRPs does not fit (capacity %llu)", (unsigned long long)n,
+                       (unsigned long long)c->cap), WW_ERR_ARG;
+    if (n) WW_CU(cudaMemcpyAsync(c->prime, host_primes, n * 8, cudaMemcpyHostToDevice, c->stream));
+    k_set_count<<<1, 1, 0, c->stream>>>(c->dc->primecount, (unsigned)n);
+    WW_CHECK_LAUNCH();
+    if (n) {
+        uint64_t blocks = (n + 255) / 256;
+        if (blocks > (uint64_t)sm_count() * 8) blocks = (uint64_t)sm_count() * 8;
+        k_fill_inverse<<<(unsigned)blocks, 256, 0, c->stream>>>(c->prime, c->inv, n);
+        WW_CHECK_LAUNCH();
+    }
+    return WW_OK;
+}
+
+int ww_marker(ww_ctx *c, int slot) {
+    if (!c || slot < 0 || slot >= 8) return set_err("bad marker slot"), WW_ERR_ARG;
+    WW_CU(cudaEventRecord(c->ev[slot], c->stream));
+    return WW_OK;
+}
+
+static int wait_event(cudaEvent_t ev, uint32_t timeout_ms) {
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return WW_OK;
+        if (e != cudaErrorNotReady) {
+            set_err("cudaEventQuery: %s", cudaGetErrorString(e));
+            return WW_ERR_CUDA;
+        }
+        const auto dt = std::chrono::steady_clock::now() - t0;
+        if (timeout_ms && std::chrono::duration_cast<std::chrono::milliseconds>(dt).count() >= timeout_ms)
+            return set_err("timed out after %u ms", timeout_ms), WW_ERR_TIMEOUT;
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+}
+
+int ww_wait_marker(ww_ctx *c, int slot, uint32_t timeout_ms) {
+    if (!c || slot < 0 || slot >= 8) return set_err("bad marker slot"), WW_ERR_ARG;
+    return wait_event(c->ev[slot], timeout_ms);
+}
+
+int ww_marker_elapsed(ww_ctx *c, int a, int b, float *ms) {
+    if (!c || a < 0 || a >= 8 || b < 0 || b >= 8 || !ms) return set_err("bad marker slot"), WW_ERR_ARG;
+    WW_CU(cudaEventElapsedTime(ms, c->ev[a], c->ev[b]));
+    return WW_OK;
+}
+
+int ww_sync(ww_ctx *c, uint32_t timeout_ms) {
+    if (!c) return set_err("null ctx"), WW_ERR_ARG;
+    WW_CU(cudaEventRecord(c->ev[7], c->stream));
+    return wait_event(c->ev[7], timeout_ms);
+}
+
+int ww_read_counters(ww_ctx *c, ww_counters *out) {
+    if (!c || !out) return set_err("null argument"), WW_ERR_ARG;
+    WW_CU(cudaMemcpyAsync(c->hc, c->dc, sizeof(DevCounters), cudaMemcpyDeviceToHost, c->stream));
+    WW_CU(cudaStreamSynchronize(c->stream));
+    out->checksum = c->hc->checksum;
+    out->total_prp_count = c->hc->total;
+    out->result_count = c->hc->resultcount;
+    out->seg_prp_count = c->hc->primecount[0];
+    out->max_prp_count = c->hc->primecount[1];
+    out->overflow = c->hc->overflow;
+    return WW_OK;
+}
+
+int ww_read_hits(ww_ctx *c, ww_hit *out, uint32_t cap, uint32_t *n) {
+    if (!c || !n || (!out && cap)) return set_err("null argument"), WW_ERR_ARG;
+    ww_counters k;
+    int rc = ww_read_counters(c, &k);
+    if (rc) return rc;
+    *n = k.result_count;
+    uint32_t m = k.result_count < c->hcap ? k.result_count : c->hcap;
+    if (m > cap) m = cap;
+    if (m) {
+        u64 *p = new (std::nothrow) u64[m];
+        int *a = new (std::nothrow) int[3 * (size_t)m];
+        if (!p || !a) {
+            delete[] p;
+            delete[] a;
+            return set_err("host allocation failed"), WW_ERR_NOMEM;
+        }
+        cudaError_t e = cudaMemcpy(p, c->hprime, (size_t)m * 8, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(a, c->hres, (size_t)m * 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(a + m, c->hrem, (size_t)m * 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(a + 2 * (size_t)m, c->hquot, (size_t)m * 4, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            delete[] p;
+            delete[] a;
+            return set_err("hit read-back: %s", cudaGetErrorString(e)), WW_ERR_CUDA;
+        }
+        for (uint32_t i = 0; i < m; ++i) {
+            out[i].p = p[i];
+            out[i].result = a[i];
+            out[i].rem = a[m + i];
+            out[i].quot = a[2 * (size_t)m + i];
+            out[i].pad = 0;
+        }
+        delete[] p;
+        delete[] a;
+    }
+    if (k.result_count > c->hcap) return set_err("%u hits, buffer holds %u", k.result_count, c->hcap),
+                                          WW_ERR_HIT_OVERFLOW;
+    return WW_OK;
+}
+
+int ww_read_prps(ww_ctx *c, uint64_t *out, uint64_t cap, uint64_t *n) {
+    if (!c || !n || (!out && cap)) return set_err("null argument"), WW_ERR_ARG;
+    ww_counters k;
+    int rc = ww_read_counters(c, &k);
+    if (rc) return rc;
+    *n = k.seg_prp_count;
+    uint64_t m = k.seg_prp_count < c->cap ? k.seg_prp_count : c->cap;
+    if (m > cap) m = cap;
+    if (m) WW_CU(cudaMemcpy(out, c->prime, m * 8, cudaMemcpyDeviceToHost));
+    if (k.seg_prp_count > c->cap) return set_err("%u PRPs, buffer holds %llu", k.seg_prp_count,
+                                                 (unsigned long long)c->cap), WW_ERR_PRP_OVERFLOW;
+    return WW_OK;
+}
+
+}  // extern "C"

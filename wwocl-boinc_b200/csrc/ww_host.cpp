@@ -1,0 +1,227 @@
+// ww_host.cpp -- host-side helpers of the reference program (main.cpp)
+// exported through the C ABI: wheel offset, primality checks of reported
+// hits, START/END parsing, result-line formatting and PRP-buffer sizing.
+#include <inttypes.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/wwcuda.h"
+#include "ww_arith.cuh"
+
+using namespace ww;
+
+namespace ww {
+void set_err(const char *fmt, ...);  // ww_capi.cu
+}
+
+namespace {
+
+bool sprp_base_host(u64 n, u64 base) {
+    const u64 q = inv64(n);
+    const u64 one = r_mod(n);
+    u64 r2 = add_mod(one, one, n);
+    r2 = add_mod(r2, r2, n);
+    for (int i = 0; i < 5; ++i) r2 = mont_mul(r2, r2, n, q);  // (4R)^(2^5) = R^2
+    const u64 nm1 = n - 1;
+    const int t = __builtin_ctzll(nm1);
+    const u64 d = nm1 >> t;
+    const u64 mb = mont_mul(base % n, r2, n, q);
+    u64 a = mb;
+    for (int i = 62 - __builtin_clzll(d); i >= 0; --i) {
+        a = mont_mul(a, a, n, q);
+        if ((d >> i) & 1) a = mont_mul(a, mb, n, q);
+    }
+    const u64 mone = n - one;
+    if (a == one || a == mone) return true;
+    for (int s = 1; s < t; ++s) {
+        a = mont_mul(a, a, n, q);
+        if (a == mone) return true;
+    }
+    return false;
+}
+
+bool hit_before(const ww_hit &a, const ww_hit &b) {
+    if (a.p != b.p) return a.p < b.p;
+    return a.result == 1093 && b.result != 1093;  // the Wieferich kernel runs first
+}
+
+}  // namespace
+
+extern "C" {
+
+int ww_find_wheel_offset(uint64_t *start, int32_t *index) {
+    if (!start || !index) return WW_ERR_ARG;
+    // first n >= start prime to 30, and its position in the gap table
+    // {4,2,4,2,4,6,2,6} that starts at residue 7 (main.cpp:528-587)
+    static const int8_t pos_of[30] = {-1, 7, -1, -1, -1, -1, -1, 0, -1, -1, -1, 1, -1, 2, -1,
+                                      -1, -1, 3, -1, 4, -1, -1, -1, 5, -1, -1, -1, -1, -1, 6};
+    uint64_t n = *start;
+    for (int k = 0; k < 7; ++k) {
+        const int i = pos_of[n % 30];
+        if (i >= 0) {
+            *start = n;
+            *index = i;
+            return WW_OK;
+        }
+        if (n == UINT64_MAX) break;
+        ++n;
+    }
+    set_err("no number >= %" PRIu64 " below 2^64 is prime to 30", *start);
+    return WW_ERR_ARG;
+}
+
+int ww_is_prime(uint64_t n) {
+    static const u64 bases[12] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+    if (n < 2) return 0;
+    if (n < 4) return 1;
+    if ((n & 1) == 0) return 0;
+    const int nb = n < 3825123056546413051ull ? 9 : 12;  // main.cpp:312-321
+    for (int i = 0; i < nb; ++i) {
+        if (n == bases[i]) return 1;
+        if (n % bases[i] == 0) return 0;
+    }
+    for (int i = 0; i < nb; ++i)
+        if (!sprp_base_host(n, bases[i])) return 0;
+    return 1;
+}
+
+int ww_is_prp(uint64_t n) {
+    static const uint32_t small[29] = {3,  5,  7,  11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53,
+                                       59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113};
+    if ((n & 1) == 0) return 0;  // main.cpp:247-280
+    for (uint32_t r : small)
+        if (n % r == 0) return 0;
+    return sprp_base_host(n, 2) ? 1 : 0;
+}
+
+int ww_parse_number(const char *s, uint64_t *out) {
+    if (!s || !out) return WW_ERR_ARG;
+    const char *e = strchr(s, 'e');
+    if (e) {  // main.cpp:1194-1221: strtoull mantissa (base 0) times 10^exp
+        char *end = nullptr;
+        uint64_t num = strtoull(s, &end, 0);
+        long exp = (end && *end) ? (long)strtoul(end + 1, nullptr, 0) : 0;
+        if (num == 0 || exp == 0) return set_err("unable to parse '%s'", s), WW_ERR_ARG;
+        for (long i = 0; i < exp; ++i) {
+            if (num > UINT64_MAX / 10) return set_err("'%s' is out of range", s), WW_ERR_ARG;
+            num *= 10;
+        }
+        *out = num;
+        return WW_OK;
+    }
+    uint64_t v = 0;
+    if (sscanf(s, "%" SCNu64, &v) != 1) return set_err("unable to parse '%s'", s), WW_ERR_ARG;
+    *out = v;
+    return WW_OK;
+}
+
+int ww_format_hits(ww_hit *hits, uint32_t n, char *buf, size_t cap, uint32_t *dropped) {
+    if ((!hits && n) || !buf || cap == 0) return WW_ERR_ARG;
+    std::stable_sort(hits, hits + n, hit_before);  // main.cpp:843-854
+    size_t off = 0;
+    uint32_t drop = 0;
+    buf[0] = '\0';
+    for (uint32_t i = 0; i < n; ++i) {
+        const ww_hit &h = hits[i];
+        char line[256];
+        if (ww_is_prime(h.p)) {  // main.cpp:869-906
+            if (h.result == 1093) {
+                if (h.rem == 1 && h.quot == 0)
+                    snprintf(line, sizeof line, "%" PRIu64 " is a Wieferich prime\n", h.p);
+                else
+                    snprintf(line, sizeof line, "%" PRIu64 " is a Wieferich special instance (%+d %+d p)\n", h.p,
+                             h.rem, h.quot);
+            } else if (h.result == 1) {
+                snprintf(line, sizeof line, "%" PRIu64 " is a WallSunSun prime\n", h.p);
+            } else if (h.result == 2) {
+                snprintf(line, sizeof line, "%" PRIu64 " is a WallSunSun special instance (+0 %+d p)\n", h.p,
+                         h.quot);
+            } else {
+                return WW_ERR_ARG;
+            }
+            const size_t len = strlen(line);
+            if (off + len + 1 > cap) return WW_ERR_ARG;
+            memcpy(buf + off, line, len + 1);
+            off += len;
+        } else if (ww_is_prp(h.p)) {
+            ++drop;  // PRP-only hit (main.cpp:907-911)
+        } else {
+            set_err("computation error, composite result %" PRIu64, h.p);
+            return WW_ERR_COMPOSITE;  // main.cpp:912-916
+        }
+    }
+    if (dropped) *dropped = drop;
+    return (int)off;
+}
+
+// Montgomery-Vaughan: pi(x+y) - pi(x) < 2y / ln y for y > 1, plus room for
+// base-2 strong pseudoprimes (very rare, and counted past the buffer end by
+// the kernels so an overflow is always detected).
+uint64_t ww_prp_count_bound(uint64_t lo, uint64_t hi) {
+    if (hi <= lo) return 0;
+    const double y = (double)(hi - lo);
+    if (y < 64) return (uint64_t)y;
+    const double b = 2.0 * y / log(y);
+    return (uint64_t)b + 1024;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Startup self-test twin (testKernels, main.cpp:590-738): the same exact
+// arithmetic as the kernels, instantiated on the host, over a short range.
+// Used only to cross-check the GPU at start-up; results are never taken
+// from it.
+
+extern "C" {
+
+int ww_selftest_digits(const uint64_t *primes, uint64_t n, uint64_t *out) {
+    if ((!primes || !out) && n) return WW_ERR_ARG;
+    for (uint64_t i = 0; i < n; ++i) {
+        const u64 p = primes[i];
+        const u64 q = inv64(p);
+        const D2 one = m2_one(p);
+        const D2 s = wieferich_digits(p, q, one);
+        const D2 c = wss_digits(p, q, one);
+        out[4 * i] = s.d0;
+        out[4 * i + 1] = s.d1;
+        out[4 * i + 2] = c.d0;
+        out[4 * i + 3] = c.d1;
+    }
+    return WW_OK;
+}
+
+int ww_selftest_range(uint64_t lo, uint64_t hi, uint64_t *prp_count, uint64_t *checksum,
+                      uint32_t *result_count) {
+    if (!prp_count || !checksum || !result_count) return WW_ERR_ARG;
+    *prp_count = 0;
+    *checksum = 0;
+    *result_count = 0;
+    if (hi <= lo) return WW_OK;
+    uint64_t n = lo | 1;  // main.cpp:649-651
+    for (; n < hi && n >= lo; n += 2) {
+        bool small = false;
+        for (uint32_t r : {3u, 5u, 7u, 11u, 13u, 17u, 19u, 23u, 29u, 31u, 37u, 41u, 43u, 47u, 53u,
+                           59u, 61u, 67u, 71u, 73u, 79u, 83u, 89u, 97u, 101u, 103u, 107u, 109u, 113u})
+            small |= (n % r == 0);
+        u64 q = 0;
+        if (small || !sprp2(n, q)) continue;  // the kernels' SPRP loop
+        const D2 one = m2_one(n);
+        const D2 s = wieferich_digits(n, q, one);
+        const D2 c = wss_digits(n, q, one);
+        ++*prp_count;
+        *checksum += (s.d1 & 0xffffffffull) + (c.d1 & 0xffffffffull);
+        int rem, quot, res;
+        *result_count += wieferich_classify(n, s, rem, quot) ? 1u : 0u;
+        *result_count += wss_classify(n, c, res, quot) ? 1u : 0u;
+        if (n > UINT64_MAX - 2) break;
+    }
+    return WW_OK;
+}
+
+}  // extern "C"

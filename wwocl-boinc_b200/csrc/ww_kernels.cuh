@@ -1,0 +1,296 @@
+// ww_kernels.cuh -- device code of the WWocl search path on sm_100a.
+//
+//   k_sieve_prp   getsegprimes (getsegprimes.cl:228-301): one CTA per segment
+//                 of 2*kSegOdd integers.  The odd numbers of the segment form a
+//                 shared-memory bitmap; each thread ORs the composite patterns
+//                 of 3..113 into its words (the reference's 27 constant tables,
+//                 getsegprimes.cl:169-225, become per-prime bit offsets kept
+//                 incrementally), then each warp compacts the survivors with
+//                 ballot/popc into a warp queue and runs the base-2 strong
+//                 PRP test 32 candidates at a time, one atomic per warp for the
+//                 output slots.
+//   k_wieferich / k_wallsunsun   the two reference test kernels.
+//   k_test_prps   both tests in one pass over the PRP list.
+//   k_digits      per-prime canonical digits (verification only).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "ww_arith.cuh"
+
+namespace ww {
+
+constexpr int kSegWords = 4096;               // bitmap words per segment (16 KB)
+constexpr int kSegOdd = kSegWords * 32;       // odd numbers per segment
+constexpr int kSieveThreads = 256;
+constexpr int kSieveWarps = kSieveThreads / 32;
+constexpr int kWordsPerThread = kSegWords / kSieveThreads;
+constexpr int kWordsPerWarp = kSegWords / kSieveWarps;
+constexpr int kQueueCap = 640;  // 31 carried + 32 words x at most 18 survivors
+constexpr int kTestThreads = 256;
+
+struct HitOut {
+    u64 *prime;
+    int *rem, *quot, *result;
+    u32 *count;
+    u32 capacity;
+    u32 *overflow;
+};
+
+__device__ __forceinline__ void emit_hit(const HitOut &h, u64 p, int result, int rem, int quot) {
+    const u32 ix = atomicAdd(h.count, 1u);
+    if (ix < h.capacity) {
+        h.prime[ix] = p;
+        h.result[ix] = result;
+        h.rem[ix] = rem;
+        h.quot[ix] = quot;
+    } else {
+        atomicOr(h.overflow, 2u);
+    }
+}
+
+__device__ __forceinline__ u64 warp_sum(u64 v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ------------------------------------------------------------------ sieve
+
+// Composite mask of one prime r for a word whose first bit is at j0 (bit j
+// of the word is the odd number n_w + 2j; r divides n_w + 2 j0).
+template <u32 R>
+__device__ __forceinline__ u32 prime_mask(u32 j0) {
+    if (R < 32) {
+        u32 pat = 0;
+#pragma unroll
+        for (u32 k = 0; k < 32; k += R) pat |= 1u << k;
+        return pat << j0;
+    }
+    return j0 < 32 ? (1u << (j0 & 31)) : 0u;
+}
+
+template <u32 R>
+__device__ __forceinline__ u32 first_hit(u64 n) {
+    // smallest j >= 0 with R | n + 2j
+    const u32 res = (u32)(n % R);
+    const u32 inv2 = (R + 1) / 2;
+    return ((R - res) % R) * inv2 % R;
+}
+
+template <u32 R>
+__device__ __forceinline__ void step_hit(u32 &j0) {
+    // next word: the index moves down by 32 (mod R)
+    const u32 d = 32 % R;
+    j0 = (j0 >= d) ? j0 - d : j0 + R - d;
+}
+
+#define WW_FOR_SMALL_PRIMES(X) \
+    X(3) X(5) X(7) X(11) X(13) X(17) X(19) X(23) X(29) X(31) X(37) X(41) X(43) X(47) X(53) \
+    X(59) X(61) X(67) X(71) X(73) X(79) X(83) X(89) X(97) X(101) X(103) X(107) X(109) X(113)
+
+struct PrpOut {
+    u64 *prime, *inv;
+    u32 *count;
+    u64 capacity;
+    u32 *overflow;
+};
+
+__device__ __forceinline__ void sprp_emit(const PrpOut &out, u64 n, bool active) {
+    u64 q = 0;
+    const bool pass = active && sprp2(n, q);
+    const u32 ballot = __ballot_sync(0xffffffffu, pass);
+    if (ballot == 0) return;
+    const int lane = threadIdx.x & 31;
+    u32 base = 0;
+    if (lane == 0) base = atomicAdd(out.count, (u32)__popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (pass) {
+        const u64 ix = (u64)base + (u64)__popc(ballot & ((1u << lane) - 1u));
+        if (ix < out.capacity) {
+            out.prime[ix] = n;
+            out.inv[ix] = q;
+        } else {
+            atomicOr(out.overflow, 1u);
+        }
+    }
+}
+
+// Sieve + SPRP over [lo, hi).  b0 = lo & ~1; segment s holds the odd numbers
+// b0 + 2(s*kSegOdd + j) + 1, j < kSegOdd.
+__global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out) {
+    __shared__ u32 bitmap[kSegWords];
+    __shared__ u32 queue[kSieveWarps][kQueueCap];
+    const u64 b0 = lo & ~1ull;
+    const u64 span = hi - b0;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+
+    for (u64 seg = blockIdx.x; seg < nseg; seg += gridDim.x) {
+        const u64 seg_off = seg * (u64)(2 * kSegOdd);
+        const u64 rem_span = span - seg_off;  // > 0
+        const u64 nvalid = (rem_span / 2 < (u64)kSegOdd) ? rem_span / 2 : (u64)kSegOdd;
+
+        // ---- pre-sieve 3..113 on this thread's contiguous words
+        {
+            const int w0 = threadIdx.x * kWordsPerThread;
+            const u64 n0 = b0 + seg_off + 64ull * (u64)w0 + 1;  // may wrap past 2^64 beyond hi
+#define WW_J0(R) u32 j##R = first_hit<R>(n0);
+            WW_FOR_SMALL_PRIMES(WW_J0)
+#undef WW_J0
+#pragma unroll 4
+            for (int w = w0; w < w0 + kWordsPerThread; ++w) {
+                u32 m = 0;
+#define WW_MASK(R) m |= prime_mask<R>(j##R); step_hit<R>(j##R);
+                WW_FOR_SMALL_PRIMES(WW_MASK)
+#undef WW_MASK
+                // bits past the end of the range are not candidates
+                const u64 first = (u64)w * 32;
+                if (first + 32 > nvalid) {
+                    const u64 keep = nvalid > first ? nvalid - first : 0;  // < 32
+                    m |= ~((1u << keep) - 1u);
+                }
+                bitmap[w] = m;
+            }
+        }
+        __syncthreads();
+
+        // ---- per-warp compaction + SPRP, 32 candidates at a time
+        u32 *q = queue[warp];
+        int qn = 0;
+        const u64 nbase = b0 + seg_off + 1;
+        for (int wb = warp * kWordsPerWarp; wb < (warp + 1) * kWordsPerWarp; wb += 32) {
+            const int w = wb + lane;
+            u32 cand = ~bitmap[w];
+            const int cnt = __popc(cand);
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            int pos = qn + incl - cnt;
+            while (cand) {
+                const int b = __ffs(cand) - 1;
+                q[pos++] = (u32)(w * 32 + b);
+                cand &= cand - 1;
+            }
+            qn += total;
+            __syncwarp();
+            while (qn >= 32) {
+                qn -= 32;
+                const u32 j = q[qn + lane];
+                __syncwarp();
+                sprp_emit(out, nbase + 2ull * j, true);
+            }
+            __syncwarp();
+        }
+        if (qn > 0) {
+            const bool act = lane < qn;
+            const u32 j = act ? q[lane] : 0u;
+            sprp_emit(out, nbase + 2ull * j, act);
+        }
+        __syncthreads();  // bitmap reused by the next segment
+    }
+}
+
+// ------------------------------------------------------------------ tests
+
+__device__ __forceinline__ void count_update(u32 *primecount, u64 *totalprimecount) {
+    // wieferich.cl:317-326: accumulate the launch's PRP count, keep the max
+    const u32 pc = primecount[0];
+    *totalprimecount += pc;
+    if (pc > primecount[1]) primecount[1] = pc;
+}
+
+__global__ void __launch_bounds__(kTestThreads) k_wieferich(u32 *primecount, const u64 *prime,
+                                                             const u64 *inv, u64 *g_one, HitOut hits,
+                                                             u64 *checksum, u64 *totalprimecount,
+                                                             u64 capacity) {
+    const u64 n = min((u64)primecount[0], capacity);
+    u64 sum = 0;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const u64 p = prime[i];
+        const u64 q = inv ? inv[i] : inv64(p);
+        const D2 one = m2_one(p);
+        if (g_one) {
+            g_one[2 * i] = one.d0;
+            g_one[2 * i + 1] = one.d1;
+        }
+        const D2 s = wieferich_digits(p, q, one);
+        sum += s.d1 & 0xffffffffull;
+        int rem, quot;
+        if (wieferich_classify(p, s, rem, quot)) emit_hit(hits, p, 1093, rem, quot);
+    }
+    sum = warp_sum(sum);
+    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(checksum, sum);
+    if (blockIdx.x == 0 && threadIdx.x == 0) count_update(primecount, totalprimecount);
+}
+
+__global__ void __launch_bounds__(kTestThreads) k_wallsunsun(const u32 *primecount, const u64 *prime,
+                                                              const u64 *inv, const u64 *g_one,
+                                                              HitOut hits, u64 *checksum, u64 capacity) {
+    const u64 n = min((u64)primecount[0], capacity);
+    u64 sum = 0;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const u64 p = prime[i];
+        const u64 q = inv ? inv[i] : inv64(p);
+        D2 one;
+        if (g_one) {
+            one.d0 = g_one[2 * i];
+            one.d1 = g_one[2 * i + 1];
+        } else {
+            one = m2_one(p);
+        }
+        const D2 c = wss_digits(p, q, one);
+        sum += c.d1 & 0xffffffffull;
+        int res, quot;
+        if (wss_classify(p, c, res, quot)) emit_hit(hits, p, res, 0, quot);
+    }
+    sum = warp_sum(sum);
+    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(checksum, sum);
+}
+
+__global__ void __launch_bounds__(kTestThreads) k_test_prps(u32 *primecount, const u64 *prime,
+                                                             const u64 *inv, HitOut hits, u64 *checksum,
+                                                             u64 *totalprimecount, u64 capacity) {
+    const u64 n = min((u64)primecount[0], capacity);
+    u64 sum = 0;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const u64 p = prime[i];
+        const u64 q = inv ? inv[i] : inv64(p);
+        const D2 one = m2_one(p);
+        const D2 s = wieferich_digits(p, q, one);
+        const D2 c = wss_digits(p, q, one);
+        sum += (s.d1 & 0xffffffffull) + (c.d1 & 0xffffffffull);
+        int rem, quot, res;
+        if (wieferich_classify(p, s, rem, quot)) emit_hit(hits, p, 1093, rem, quot);
+        if (wss_classify(p, c, res, quot)) emit_hit(hits, p, res, 0, quot);
+    }
+    sum = warp_sum(sum);
+    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(checksum, sum);
+    if (blockIdx.x == 0 && threadIdx.x == 0) count_update(primecount, totalprimecount);
+}
+
+__global__ void k_digits(const u64 *primes, u64 n, u64 *out) {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const u64 p = primes[i];
+        const u64 q = inv64(p);
+        const D2 one = m2_one(p);
+        const D2 s = wieferich_digits(p, q, one);
+        const D2 c = wss_digits(p, q, one);
+        out[4 * i] = s.d0;
+        out[4 * i + 1] = s.d1;
+        out[4 * i + 2] = c.d0;
+        out[4 * i + 3] = c.d1;
+    }
+}
+
+// q = p^-1 mod 2^64 for a loaded list; sets the segment count.
+__global__ void k_fill_inverse(const u64 *prime, u64 *inv, u64 n) {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        inv[i] = inv64(prime[i]);
+}
+
+}  // namespace ww

@@ -1,0 +1,330 @@
+"""ctypes binding of libwwcuda.so (include/wwcuda.h) for Python callers.
+
+This is the Python face of the C ABI that the wwocl host program uses; the
+tests and the benchmark drive the CUDA path through it.  There is no CPU
+fallback: importing this module fails when the shared library is missing,
+and every call raises WWError on a non-zero status.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libwwcuda.so"
+
+if not LIB_PATH.exists():
+    raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {PKG}` (no CPU fallback exists)")
+
+_L = C.CDLL(str(LIB_PATH))
+
+WW_OK = 0
+STATUS = {0: "ok", -1: "cuda", -2: "arg", -3: "prp_overflow", -4: "hit_overflow", -5: "timeout",
+          -6: "nomem", -7: "composite", -8: "state", -9: "nodev"}
+
+
+class WWError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = _L.ww_last_error().decode(errors="replace")
+        super().__init__(f"{where}: {STATUS.get(status, status)} ({msg})")
+        self.status = status
+
+
+class Hit(C.Structure):
+    _fields_ = [("p", C.c_uint64), ("result", C.c_int32), ("rem", C.c_int32),
+                ("quot", C.c_int32), ("pad", C.c_int32)]
+
+
+class Counters(C.Structure):
+    _fields_ = [("checksum", C.c_uint64), ("total_prp_count", C.c_uint64),
+                ("result_count", C.c_uint32), ("seg_prp_count", C.c_uint32),
+                ("max_prp_count", C.c_uint32), ("overflow", C.c_uint32)]
+
+
+class Buffers(C.Structure):
+    _fields_ = [("prime", C.c_void_p), ("invert", C.c_void_p), ("one", C.c_void_p),
+                ("special_prime", C.c_void_p), ("rem", C.c_void_p), ("quot", C.c_void_p),
+                ("result", C.c_void_p), ("checksum", C.c_void_p), ("total_prp_count", C.c_void_p),
+                ("result_count", C.c_void_p), ("primecount", C.c_void_p), ("overflow", C.c_void_p),
+                ("prp_capacity", C.c_uint64), ("hit_capacity", C.c_uint32), ("stream", C.c_void_p)]
+
+
+_U64P = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+_VP = C.c_void_p
+_SIGS = {
+    "ww_last_error": (C.c_char_p, []),
+    "ww_status_string": (C.c_char_p, [C.c_int]),
+    "ww_abi_version": (C.c_int, []),
+    "ww_launch_clearn": (C.c_int, [_VP, _VP]),
+    "ww_launch_clearresult": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "ww_launch_getsegprimes": (C.c_int, [C.c_uint64, C.c_uint64, C.c_int32, _VP, _VP, _VP, C.c_uint64,
+                                         _VP, _VP]),
+    "ww_launch_wieferich": (C.c_int, [_VP] * 11 + [C.c_uint64, C.c_uint32, _VP, _VP]),
+    "ww_launch_wallsunsun": (C.c_int, [_VP] * 10 + [C.c_uint64, C.c_uint32, _VP, _VP]),
+    "ww_launch_test_prps": (C.c_int, [_VP] * 10 + [C.c_uint64, C.c_uint32, _VP, _VP]),
+    "ww_launch_digits": (C.c_int, [_VP, C.c_uint64, _VP, _VP]),
+    "ww_open": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "ww_close": (None, [_VP]),
+    "ww_reserve": (C.c_int, [_VP, C.c_uint64, C.c_uint32]),
+    "ww_clear_results": (C.c_int, [_VP]),
+    "ww_clear_segment": (C.c_int, [_VP]),
+    "ww_sieve_prp": (C.c_int, [_VP, C.c_uint64, C.c_uint64, C.c_int32]),
+    "ww_wieferich": (C.c_int, [_VP]),
+    "ww_wallsunsun": (C.c_int, [_VP]),
+    "ww_test_prps": (C.c_int, [_VP]),
+    "ww_load_prps": (C.c_int, [_VP, _VP, C.c_uint64]),
+    "ww_marker": (C.c_int, [_VP, C.c_int]),
+    "ww_wait_marker": (C.c_int, [_VP, C.c_int, C.c_uint32]),
+    "ww_marker_elapsed": (C.c_int, [_VP, C.c_int, C.c_int, C.POINTER(C.c_float)]),
+    "ww_sync": (C.c_int, [_VP, C.c_uint32]),
+    "ww_read_counters": (C.c_int, [_VP, C.POINTER(Counters)]),
+    "ww_read_hits": (C.c_int, [_VP, C.POINTER(Hit), C.c_uint32, C.POINTER(C.c_uint32)]),
+    "ww_read_prps": (C.c_int, [_VP, _VP, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "ww_get_buffers": (C.c_int, [_VP, C.POINTER(Buffers)]),
+    "ww_find_wheel_offset": (C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_int32)]),
+    "ww_is_prime": (C.c_int, [C.c_uint64]),
+    "ww_is_prp": (C.c_int, [C.c_uint64]),
+    "ww_parse_number": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint64)]),
+    "ww_format_hits": (C.c_int, [C.POINTER(Hit), C.c_uint32, C.c_char_p, C.c_size_t,
+                                 C.POINTER(C.c_uint32)]),
+    "ww_prp_count_bound": (C.c_uint64, [C.c_uint64, C.c_uint64]),
+    "ww_selftest_digits": (C.c_int, [_U64P, C.c_uint64, _U64P]),
+    "ww_selftest_range": (C.c_int, [C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64),
+                                    C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
+    "ww_random_primes": (C.c_int, [C.c_int, C.c_uint64, C.c_uint64, _U64P, C.POINTER(C.c_uint64)]),
+    "ww_pipe_bench": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+}
+for _name, (_res, _args) in _SIGS.items():
+    _f = getattr(_L, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+def lib() -> C.CDLL:
+    return _L
+
+
+def check(rc: int, where: str) -> int:
+    if rc < 0:
+        raise WWError(rc, where)
+    return rc
+
+
+# ----------------------------------------------------------------- host helpers
+
+def find_wheel_offset(start: int) -> tuple[int, int]:
+    s = C.c_uint64(start)
+    i = C.c_int32(0)
+    check(_L.ww_find_wheel_offset(C.byref(s), C.byref(i)), "ww_find_wheel_offset")
+    return int(s.value), int(i.value)
+
+
+def is_prime(n: int) -> bool:
+    return bool(_L.ww_is_prime(n))
+
+
+def is_prp(n: int) -> bool:
+    return bool(_L.ww_is_prp(n))
+
+
+def parse_number(text: str) -> int:
+    v = C.c_uint64(0)
+    check(_L.ww_parse_number(text.encode(), C.byref(v)), f"ww_parse_number({text!r})")
+    return int(v.value)
+
+
+def format_hits(hits: list[tuple[int, int, int, int]]) -> tuple[str, int]:
+    arr = (Hit * max(len(hits), 1))()
+    for i, (p, r, rem, q) in enumerate(hits):
+        arr[i].p, arr[i].result, arr[i].rem, arr[i].quot = p, r, rem, q
+    buf = C.create_string_buffer(256 * max(len(hits), 1) + 1)
+    dropped = C.c_uint32(0)
+    check(_L.ww_format_hits(arr, len(hits), buf, len(buf), C.byref(dropped)), "ww_format_hits")
+    return buf.value.decode(), int(dropped.value)
+
+
+def prp_count_bound(lo: int, hi: int) -> int:
+    return int(_L.ww_prp_count_bound(lo, hi))
+
+
+def selftest_digits(primes: np.ndarray) -> np.ndarray:
+    primes = np.ascontiguousarray(primes, dtype=np.uint64)
+    out = np.zeros(4 * primes.size, dtype=np.uint64)
+    check(_L.ww_selftest_digits(primes, primes.size, out), "ww_selftest_digits")
+    return out.reshape(-1, 4)
+
+
+def selftest_range(lo: int, hi: int) -> dict:
+    a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint32()
+    check(_L.ww_selftest_range(lo, hi, C.byref(a), C.byref(b), C.byref(c)), "ww_selftest_range")
+    return dict(prp_count=a.value, checksum=b.value, result_count=c.value)
+
+
+def random_primes(seed: int, n: int, device: int = 0) -> tuple[np.ndarray, int]:
+    out = np.zeros(n, dtype=np.uint64)
+    used = C.c_uint64(0)
+    check(_L.ww_random_primes(device, seed, n, out, C.byref(used)), "ww_random_primes")
+    return out, int(used.value)
+
+
+def pipe_bench(mode: int, device: int = 0) -> tuple[float, float]:
+    ops, ms = C.c_double(0), C.c_double(0)
+    check(_L.ww_pipe_bench(device, mode, C.byref(ops), C.byref(ms)), "ww_pipe_bench")
+    return ops.value, ms.value
+
+
+# -------------------------------------------------------------------- context
+
+class Context:
+    """Owns a ww_ctx: stream, PRP buffers, hit buffers, counters."""
+
+    def __init__(self, device: int = 0, max_prps: int = 1 << 20, max_hits: int = 15000):
+        h = C.c_void_p()
+        check(_L.ww_open(device, C.byref(h)), "ww_open")
+        self.h = h
+        self.device = device
+        self.reserve(max_prps, max_hits)
+
+    def close(self) -> None:
+        if self.h:
+            _L.ww_close(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reserve(self, max_prps: int, max_hits: int = 15000) -> None:
+        check(_L.ww_reserve(self.h, max_prps, max_hits), "ww_reserve")
+        self.max_prps, self.max_hits = max_prps, max_hits
+
+    def clear_results(self):
+        check(_L.ww_clear_results(self.h), "ww_clear_results")
+
+    def clear_segment(self):
+        check(_L.ww_clear_segment(self.h), "ww_clear_segment")
+
+    def sieve_prp(self, start: int, stop: int) -> None:
+        """getsegprimes over [start, stop) after the wheel alignment of start."""
+        ks, idx = find_wheel_offset(start)
+        if ks >= stop:
+            return
+        check(_L.ww_sieve_prp(self.h, ks, stop, idx), "ww_sieve_prp")
+
+    def wieferich(self):
+        check(_L.ww_wieferich(self.h), "ww_wieferich")
+
+    def wallsunsun(self):
+        check(_L.ww_wallsunsun(self.h), "ww_wallsunsun")
+
+    def test_prps(self):
+        check(_L.ww_test_prps(self.h), "ww_test_prps")
+
+    def load_prps(self, primes: np.ndarray) -> None:
+        primes = np.ascontiguousarray(primes, dtype=np.uint64)
+        check(_L.ww_load_prps(self.h, primes.ctypes.data, primes.size), "ww_load_prps")
+
+    def load_prps_ptr(self, host_ptr: int, n: int) -> None:
+        check(_L.ww_load_prps(self.h, host_ptr, n), "ww_load_prps")
+
+    def sync(self, timeout_ms: int = 600_000):
+        check(_L.ww_sync(self.h, timeout_ms), "ww_sync")
+
+    def marker(self, slot: int):
+        check(_L.ww_marker(self.h, slot), "ww_marker")
+
+    def wait_marker(self, slot: int, timeout_ms: int = 600_000):
+        check(_L.ww_wait_marker(self.h, slot, timeout_ms), "ww_wait_marker")
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        ms = C.c_float(0)
+        check(_L.ww_marker_elapsed(self.h, a, b, C.byref(ms)), "ww_marker_elapsed")
+        return float(ms.value)
+
+    def counters(self) -> dict:
+        k = Counters()
+        check(_L.ww_read_counters(self.h, C.byref(k)), "ww_read_counters")
+        return dict(checksum=k.checksum, total_prp_count=k.total_prp_count, result_count=k.result_count,
+                    seg_prp_count=k.seg_prp_count, max_prp_count=k.max_prp_count, overflow=k.overflow)
+
+    def hits(self) -> list[tuple[int, int, int, int]]:
+        cap = self.max_hits
+        arr = (Hit * cap)()
+        n = C.c_uint32(0)
+        check(_L.ww_read_hits(self.h, arr, cap, C.byref(n)), "ww_read_hits")
+        return [(arr[i].p, arr[i].result, arr[i].rem, arr[i].quot) for i in range(min(n.value, cap))]
+
+    def prps(self) -> np.ndarray:
+        cnt = self.counters()["seg_prp_count"]
+        out = np.zeros(max(min(cnt, self.max_prps), 1), dtype=np.uint64)
+        n = C.c_uint64(0)
+        check(_L.ww_read_prps(self.h, out.ctypes.data, out.size, C.byref(n)), "ww_read_prps")
+        return out[: min(n.value, out.size)]
+
+    def buffers(self) -> Buffers:
+        b = Buffers()
+        check(_L.ww_get_buffers(self.h, C.byref(b)), "ww_get_buffers")
+        return b
+
+    # one-shot helpers ---------------------------------------------------
+    def run_range(self, lo: int, hi: int, fused: bool = True, segment: int | None = None) -> dict:
+        """Plain path over [lo, hi): clear, then per segment clearn -> sieve -> tests."""
+        self.clear_results()
+        seg = segment or hi - lo
+        start = lo
+        while start < hi:
+            stop = min(start + seg, hi)
+            self.clear_segment()
+            self.sieve_prp(start, stop)
+            if fused:
+                self.test_prps()
+            else:
+                self.wieferich()
+                self.wallsunsun()
+            start = stop
+        self.sync()
+        c = self.counters()
+        c["hits"] = self.hits()
+        return c
+
+
+def digits(primes: np.ndarray, device: int = 0) -> np.ndarray:
+    """Per-prime (s0, s1, c20, c21) on the GPU via ww_launch_digits (torch for device memory)."""
+    import torch
+
+    primes = np.ascontiguousarray(primes, dtype=np.uint64)
+    dev = torch.device("cuda", device)
+    p = torch.from_numpy(primes.view(np.int64)).to(dev)
+    out = torch.empty(4 * primes.size, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    check(_L.ww_launch_digits(p.data_ptr(), primes.size, out.data_ptr(), stream), "ww_launch_digits")
+    torch.cuda.synchronize(dev)
+    return out.cpu().numpy().view(np.uint64).reshape(-1, 4)
+
+
+def exported_symbols() -> list[str]:
+    return sorted(_SIGS)
+
+
+def header_symbols(header: Path | None = None) -> list[str]:
+    import re
+
+    header = header or PKG.parent / "include" / "wwcuda.h"
+    text = header.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ww_[a-z0-9_]+)\s*\(", text)))
+
+
+if os.environ.get("WW_DEBUG_IMPORT"):
+    print("libwwcuda loaded from", LIB_PATH)
