@@ -219,6 +219,11 @@ uint64_t ww_prp_count_bound(uint64_t lo, uint64_t hi);
 int ww_selftest_digits(const uint64_t *primes, uint64_t n, uint64_t *out);
 int ww_selftest_range(uint64_t lo, uint64_t hi, uint64_t *prp_count, uint64_t *checksum,
                       uint32_t *result_count);
+/* One operation of the kernels' mod p^2 arithmetic on the host, for
+ * checking it operand by operand: op 0 = X*Y/2^64, 1 = X^2/2^64,
+ * 2 = X/2^64 (mod p^2), inputs and outputs as digit pairs x0 + p x1;
+ * xy = (x0, x1, y0, y1) per case, out = (z0, z1). */
+int ww_selftest_m2(int op, uint64_t p, const uint64_t *xy, uint64_t n, uint64_t *out);
 
 /* ---------------------------------------------------------------------------
  * 4. Measurement utilities (no reference counterpart).

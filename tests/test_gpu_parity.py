@@ -1,0 +1,194 @@
+"""CUDA path against the oracle and the reference fixtures, through the C ABI.
+
+Bit-exact everywhere: PRP sets (digests of the sorted list), per-prime
+digits, checksums, hit records and counts."""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import sample_names
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(ww):
+    c = ww.Context(0, max_prps=1 << 22, max_hits=15000)
+    yield c
+    c.close()
+
+
+def test_digits_kernel_matches_oracle(ww, oracle, ref_terms):
+    for name in sample_names(ref_terms):
+        ps = ref_terms[name + "_p"]
+        d = ww.digits(ps)
+        w, s = oracle.list_digits(ps)
+        assert np.array_equal(d[:, 0:2], w), name
+        assert np.array_equal(d[:, 2:4], s), name
+        assert np.array_equal((d[:, 1] & 0xFFFFFFFF).astype(np.uint32), ref_terms[name + "_wterm"]), name
+        assert np.array_equal((d[:, 3] & 0xFFFFFFFF).astype(np.uint32), ref_terms[name + "_sterm"]), name
+
+
+def test_digits_kernel_random_list(ww, oracle):
+    ps, _ = oracle.random_primes(7, 1 << 14)
+    d = ww.digits(ps)
+    w, s = oracle.list_digits(ps)
+    assert np.array_equal(d[:, 0:2], w) and np.array_equal(d[:, 2:4], s)
+
+
+def test_random_prime_list_matches_oracle(ww, oracle):
+    got, used = ww.random_primes(7, 5000)
+    want, used_o = oracle.random_primes(7, 5000)
+    assert np.array_equal(got, want) and used == used_o
+
+
+def _digest(arr):
+    arr = np.sort(np.asarray(arr, dtype=np.uint64))
+    return arr.size, int(arr.sum(dtype=np.uint64)), hashlib.sha256(arr.astype("<u8").tobytes()).hexdigest()
+
+
+def test_sieve_prp_sets_match_reference(ctx, ref_prps):
+    for name, r in ref_prps.items():
+        ctx.clear_results()
+        ctx.clear_segment()
+        ctx.sieve_prp(r["lo"], r["hi"])
+        ctx.sync()
+        c = ctx.counters()
+        assert c["overflow"] == 0, name
+        lst = ctx.prps()
+        assert _digest(lst) == (r["count"], r["sum_mod_2_64"], r["sha256"]), name
+
+
+def test_sieve_prp_list_inverse(ww):
+    """g_invert holds p^-1 mod 2^64 for each listed p (getsegprimes.cl:291-296)."""
+    import torch
+
+    L = ww.lib()
+    dev = torch.device("cuda", 0)
+    cap = 1 << 16
+    prime = torch.zeros(cap, dtype=torch.int64, device=dev)
+    inv = torch.zeros(cap, dtype=torch.int64, device=dev)
+    pc = torch.zeros(2, dtype=torch.int32, device=dev)
+    ovf = torch.zeros(1, dtype=torch.int32, device=dev)
+    lo, idx = ww.find_wheel_offset(2**64 - 10**6 - 1)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    ww.check(L.ww_launch_getsegprimes(lo, 2**64 - 1, idx, prime.data_ptr(), inv.data_ptr(), pc.data_ptr(), cap,
+                                      ovf.data_ptr(), st), "getsegprimes")
+    torch.cuda.synchronize(dev)
+    n = int(pc[0].item())
+    assert n > 20000 and int(ovf.item()) == 0
+    p = prime[:n].cpu().numpy().view(np.uint64)
+    q = inv[:n].cpu().numpy().view(np.uint64)
+    with np.errstate(over="ignore"):
+        assert np.all(p * q == np.uint64(1))
+
+
+@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("name", ["small_3e6", "cross_2p32", "near_top_2e6", "wieferich_special_window",
+                                  "wss_special_window", "mid_2p48", "config1_5e7", "top_1e8"])
+def test_pipeline_matches_reference(ctx, ref_ranges, name, fused):
+    r = ref_ranges[name]
+    got = ctx.run_range(r["lo"], r["hi"], fused=fused)
+    assert got["overflow"] == 0
+    assert got["total_prp_count"] == r["prp_count"]
+    assert "%016X" % got["checksum"] == r["checksum"]
+    assert got["result_count"] == r["cpu_results"]
+
+
+def test_segmented_run_equals_whole(ctx, ref_ranges):
+    r = ref_ranges["small_3e6"]
+    a = ctx.run_range(r["lo"], r["hi"], segment=123_457)
+    assert "%016X" % a["checksum"] == r["checksum"]
+    assert a["total_prp_count"] == r["prp_count"]
+    assert a["max_prp_count"] < r["prp_count"]
+
+
+def test_hits_match_oracle(ctx, oracle):
+    lo, hi = 127, 2_000_000
+    got = ctx.run_range(lo, hi)
+    _, _, want = oracle.scan_range(lo, hi, hit_cap=100000)
+    assert sorted(got["hits"]) == sorted(want)
+
+
+def test_prp_overflow_is_reported(ww, oracle):
+    with ww.Context(0, max_prps=1000, max_hits=100) as c:
+        c.clear_results()
+        c.clear_segment()
+        c.sieve_prp(127, 1_000_000)
+        c.sync()
+        k = c.counters()
+        summ, _, _ = oracle.scan_range(127, 1_000_000)
+        assert k["overflow"] & 1 and k["seg_prp_count"] == summ["prp_count"]
+        with pytest.raises(ww.WWError) as e:
+            c.prps()
+        assert e.value.status == -3
+
+
+def test_hit_overflow_is_reported(ww):
+    with ww.Context(0, max_prps=1 << 20, max_hits=10) as c:
+        got = c.run_range(127, 1_000_000)
+        assert got["overflow"] & 2 and got["result_count"] > 10
+        with pytest.raises(ww.WWError) as e:
+            c.hits()
+        assert e.value.status == -4
+
+
+def test_kernel_shaped_launchers_on_torch_memory(ww, ref_ranges):
+    """The reference kernel sequence clearresult, clearn, getsegprimes,
+    wieferich, wallsunsun on caller-owned device memory and stream."""
+    import torch
+
+    L = ww.lib()
+    r = ref_ranges["cross_2p32"]
+    dev = torch.device("cuda", 0)
+    cap, nres = 1 << 18, 15000
+    prime = torch.empty(cap, dtype=torch.int64, device=dev)
+    inv = torch.empty(cap, dtype=torch.int64, device=dev)
+    one = torch.empty(2 * cap, dtype=torch.int64, device=dev)
+    sp = torch.empty(nres, dtype=torch.int64, device=dev)
+    rem = torch.empty(nres, dtype=torch.int32, device=dev)
+    quot = torch.empty(nres, dtype=torch.int32, device=dev)
+    res = torch.empty(nres, dtype=torch.int32, device=dev)
+    cks = torch.zeros(1, dtype=torch.int64, device=dev)
+    total = torch.zeros(1, dtype=torch.int64, device=dev)
+    rc = torch.zeros(1, dtype=torch.int32, device=dev)
+    pc = torch.zeros(2, dtype=torch.int32, device=dev)
+    ovf = torch.zeros(1, dtype=torch.int32, device=dev)
+    s = torch.cuda.Stream(dev)
+    st = s.cuda_stream
+    P = lambda t: t.data_ptr()  # noqa: E731
+    start, idx = ww.find_wheel_offset(r["lo"])
+    ww.check(L.ww_launch_clearresult(P(cks), P(rc), P(total), P(pc), st), "clearresult")
+    ww.check(L.ww_launch_clearn(P(pc), st), "clearn")
+    ww.check(L.ww_launch_getsegprimes(start, r["hi"], idx, P(prime), P(inv), P(pc), cap, P(ovf), st), "gsp")
+    ww.check(L.ww_launch_wieferich(P(pc), P(prime), P(inv), P(one), P(sp), P(rem), P(quot), P(res), P(cks),
+                                   P(rc), P(total), cap, nres, P(ovf), st), "wieferich")
+    ww.check(L.ww_launch_wallsunsun(P(pc), P(prime), P(inv), P(one), P(sp), P(rem), P(quot), P(res), P(cks),
+                                    P(rc), cap, nres, P(ovf), st), "wallsunsun")
+    s.synchronize()
+    assert int(ovf.item()) == 0
+    assert int(total.item()) == r["prp_count"]
+    assert "%016X" % (int(cks.item()) % 2**64) == r["checksum"]
+    assert int(rc.item()) == r["cpu_results"]
+
+
+def test_bad_arguments_are_rejected(ww):
+    with ww.Context(0, max_prps=1024, max_hits=16) as c:
+        L = ww.lib()
+        # wheel index that does not belong to the start
+        assert L.ww_sieve_prp(c.h, 127, 1000, 3) == -2
+        # start below 127 (main.cpp:1265-1269 clamps; the kernel refuses)
+        assert L.ww_sieve_prp(c.h, 121, 1000, 7) == -2
+        # empty range
+        assert L.ww_sieve_prp(c.h, 127, 127, 0) == -2
+        c.sync()
+        assert c.counters()["seg_prp_count"] == 0
+
+
+def test_pipe_bench_runs(ww):
+    for mode in range(6):
+        ops, ms = ww.pipe_bench(mode)
+        assert ops > 1e11 and ms > 0

@@ -117,3 +117,41 @@ def test_format_hits_matches_oracle(ww, oracle):
 def test_prp_bound_covers_fixtures(ww, ref_ranges):
     for r in ref_ranges.values():
         assert ww.prp_count_bound(r["lo"], r["hi"]) >= r["prp_count"]
+
+
+def _m2_exact(op, p, x0, x1, y0, y1):
+    n = p * p
+    rinv = pow(2**64, -1, n)
+    x, y = x0 + p * x1, y0 + p * y1
+    z = (x * y if op == 0 else x * x if op == 1 else x) * rinv % n
+    return z % p, z // p
+
+
+def test_m2_arithmetic_edge_cases(ww):
+    """The 32-bit carry-chain products (the instruction sequence the kernels
+    run) against exact integer arithmetic, operand by operand, including
+    the digits 0, 1, p-1 and moduli at the 2^32, 2^63 and 2^64 edges."""
+    rng = np.random.default_rng(3)
+    mods = [127, 131, 65521, 2**31 - 1, 4294967291, 4294967311, 2**32 + 15, 2**61 - 1, 2**62 + 135,
+            9223372036854775783, 2**63 + 29, 2**64 - 59, 2**64 - 1, 2**64 - 3, 12297829382473034411]
+    for p in mods:
+        special = sorted({0, 1, 2, p - 1, p - 2, p // 2, (p + 1) // 2, 2**32 % p, (2**32 - 1) % p, p - 2**31 % p}
+                         | {int(v) % p for v in rng.integers(0, 2**63, 6, dtype=np.uint64)})
+        cases = [(a, b, c, d) for a in special for b in special[:6] for c in special[:6] for d in special]
+        xy = np.array(cases, dtype=np.uint64)
+        for op in (0, 1, 2):
+            got = ww.selftest_m2(op, p, xy)
+            want = [_m2_exact(op, p, *c) for c in cases]
+            assert [tuple(map(int, g)) for g in got] == want, (p, op)
+
+
+def test_m2_arithmetic_random(ww):
+    rng = np.random.default_rng(4)
+    for _ in range(40):
+        p = int(rng.integers(2**40, 2**64 - 1, dtype=np.uint64)) | 1
+        cases = [tuple(int(v) % p for v in rng.integers(0, 2**64 - 1, 4, dtype=np.uint64)) for _ in range(500)]
+        xy = np.array(cases, dtype=np.uint64)
+        for op in (0, 1, 2):
+            got = ww.selftest_m2(op, p, xy)
+            want = [_m2_exact(op, p, *c) for c in cases]
+            assert [tuple(map(int, g)) for g in got] == want, (p, op)

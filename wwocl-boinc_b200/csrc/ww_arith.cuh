@@ -238,104 +238,4 @@ WW_HD D2 m2_div5(D2 t, u64 p) {
     return y;
 }
 
-// ------------------------------------------------------------ the two tests
-
-// 2^((p-1)/2) mod p^2 as canonical digits (wieferich.cl:219-245).
-WW_HD D2 wieferich_digits(u64 p, u64 q, D2 one) {
-    const u64 e = p >> 1;
-#if defined(__CUDA_ARCH__)
-    const int top = 63 - __clzll((long long)e);
-#else
-    const int top = 63 - __builtin_clzll(e);
-#endif
-    D2 a = m2_dbl(one, p);
-    for (int i = top - 1; i >= 0; --i) {
-        a = m2_sqr(a, p, q);
-        const D2 d = m2_dbl(a, p);
-        const bool bit = (e >> i) & 1;
-        a.d0 = bit ? d.d0 : a.d0;
-        a.d1 = bit ? d.d1 : a.d1;
-    }
-    return m2_redc(a, p, q);
-}
-
-// F_{p-(p|5)} mod p^2 as canonical digits.  The reference walks the
-// (F_k, F_{k-1}) doubling ladder, two squarings and a product per bit
-// (wallsunsun.cl:242-300).  Here the Lucas numbers V_k = L_k run a
-// Montgomery ladder (V_k, V_{k+1}), one squaring and one product per bit:
-//   V_2k = V_k^2 - 2(-1)^k,  V_2k+1 = V_k V_k+1 - (-1)^k,
-//   V_2k+2 = V_k+1^2 + 2(-1)^k,
-// and F_n = (2 V_{n+1} - V_n) / 5 gives the same residue exactly.
-WW_HD D2 wss_digits(u64 p, u64 q, D2 one) {
-    const u32 pm5 = (u32)(p % 5);
-    const u64 n = (pm5 == 2 || pm5 == 3) ? p + 1 : p - 1;  // p - (p|5)
-#if defined(__CUDA_ARCH__)
-    const int top = 63 - __clzll((long long)n);
-#else
-    const int top = 63 - __builtin_clzll(n);
-#endif
-    const D2 zero = {0, 0};
-    const D2 two = m2_dbl(one, p);
-    const D2 mone = m2_sub(zero, one, p);
-    const D2 mtwo = m2_sub(zero, two, p);
-    D2 A = one;                 // V_1
-    D2 B = m2_add(two, one, p); // V_2
-    bool odd = true;            // parity of the ladder index k
-    for (int i = top - 1; i >= 0; --i) {
-        const bool bit = (n >> i) & 1;
-        D2 s;
-        s.d0 = bit ? B.d0 : A.d0;
-        s.d1 = bit ? B.d1 : A.d1;
-        const D2 sq = m2_sqr(s, p, q);
-        const D2 pr = m2_mul(A, B, p, q);
-        // pr - (-1)^k ; sq -/+ 2(-1)^k
-        D2 cp, cs;
-        cp.d0 = odd ? one.d0 : mone.d0;
-        cp.d1 = odd ? one.d1 : mone.d1;
-        const bool plus2 = bit ^ odd;  // bit=0: -2(-1)^k, bit=1: +2(-1)^k
-        cs.d0 = plus2 ? two.d0 : mtwo.d0;
-        cs.d1 = plus2 ? two.d1 : mtwo.d1;
-        const D2 np = m2_add(pr, cp, p);
-        const D2 ns = m2_add(sq, cs, p);
-        A.d0 = bit ? np.d0 : ns.d0;
-        A.d1 = bit ? np.d1 : ns.d1;
-        B.d0 = bit ? ns.d0 : np.d0;
-        B.d1 = bit ? ns.d1 : np.d1;
-        odd = bit;
-    }
-    const D2 t = m2_redc(m2_sub(m2_dbl(B, p), A, p), p, q);
-    return m2_div5(t, p);
-}
-
-// ------------------------------------------------------------ classification
-
-constexpr u64 kThreshold = 1000;  // WW.h:8 SPECIAL_THRESHOLD
-
-// wieferich.cl:248-293.  Returns true and fills rem/quot for a hit.
-WW_HD bool wieferich_classify(u64 p, D2 s, int &rem, int &quot) {
-    if (((s.d1 == 0) & (s.d0 == 1)) | ((s.d1 == p - 1) & (s.d0 == p - 1))) {
-        rem = 1;
-        quot = 0;
-        return true;
-    }
-    if (s.d1 <= kThreshold) {
-        if (s.d0 == 1) { rem = 1; quot = (int)s.d1; return true; }
-        if (s.d0 == p - 1) { rem = -1; quot = (int)(s.d1 + 1); return true; }
-        return false;
-    }
-    if (s.d1 >= p - kThreshold) {
-        if (s.d0 == 1) { rem = 1; quot = (int)(s.d1 - p); return true; }
-        if (s.d0 == p - 1) { rem = -1; quot = (int)(s.d1 + 1 - p); return true; }
-    }
-    return false;
-}
-
-// wallsunsun.cl:325-349.  result 1 = WSS prime, 2 = special instance.
-WW_HD bool wss_classify(u64 p, D2 c, int &result, int &quot) {
-    if (c.d1 == 0) { result = 1; quot = 0; return true; }
-    if (c.d1 <= kThreshold) { result = 2; quot = (int)c.d1; return true; }
-    if (c.d1 >= p - kThreshold) { result = 2; quot = (int)(c.d1 - p); return true; }
-    return false;
-}
-
 }  // namespace ww

@@ -11,7 +11,7 @@
 #include <vector>
 
 #include "../../include/wwcuda.h"
-#include "ww_arith.cuh"
+#include "ww_tests.cuh"
 
 using namespace ww;
 
@@ -186,8 +186,8 @@ int ww_selftest_digits(const uint64_t *primes, uint64_t n, uint64_t *out) {
         const u64 p = primes[i];
         const u64 q = inv64(p);
         const D2 one = m2_one(p);
-        const D2 s = wieferich_digits(p, q, one);
-        const D2 c = wss_digits(p, q, one);
+        D2 s, c;
+        both_digits(p, q, one, s, c);
         out[4 * i] = s.d0;
         out[4 * i + 1] = s.d1;
         out[4 * i + 2] = c.d0;
@@ -210,7 +210,7 @@ int ww_selftest_range(uint64_t lo, uint64_t hi, uint64_t *prp_count, uint64_t *c
                            59u, 61u, 67u, 71u, 73u, 79u, 83u, 89u, 97u, 101u, 103u, 107u, 109u, 113u})
             small |= (n % r == 0);
         u64 q = 0;
-        if (small || !sprp2(n, q)) continue;  // the kernels' SPRP loop
+        if (small || !prp_test(n, q)) continue;  // the kernels' SPRP loop
         const D2 one = m2_one(n);
         const D2 s = wieferich_digits(n, q, one);
         const D2 c = wss_digits(n, q, one);
@@ -225,3 +225,21 @@ int ww_selftest_range(uint64_t lo, uint64_t hi, uint64_t *prp_count, uint64_t *c
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Operation-level check of the two-digit arithmetic the kernels run (host
+// instantiation of the same source): op 0 product, 1 square, 2 leave
+// Montgomery form.  xy holds (x0, x1, y0, y1) per case, out (z0, z1).
+
+extern "C" int ww_selftest_m2(int op, uint64_t p, const uint64_t *xy, uint64_t n, uint64_t *out) {
+    if ((p & 1) == 0 || p < 3 || ((!xy || !out) && n) || op < 0 || op > 2) return WW_ERR_ARG;
+    const Arith32 ar(p, inv64(p));
+    for (uint64_t i = 0; i < n; ++i) {
+        const D2 x = {xy[4 * i], xy[4 * i + 1]};
+        const D2 y = {xy[4 * i + 2], xy[4 * i + 3]};
+        const D2 z = op == 0 ? ar.mul(x, y) : op == 1 ? ar.sqr(x) : ar.redc(x);
+        out[2 * i] = z.d0;
+        out[2 * i + 1] = z.d1;
+    }
+    return WW_OK;
+}

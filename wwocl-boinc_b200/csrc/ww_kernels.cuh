@@ -16,7 +16,7 @@
 
 #include <cuda_runtime.h>
 
-#include "ww_arith.cuh"
+#include "ww_tests.cuh"
 
 namespace ww {
 
@@ -98,7 +98,7 @@ struct PrpOut {
 
 __device__ __forceinline__ void sprp_emit(const PrpOut &out, u64 n, bool active) {
     u64 q = 0;
-    const bool pass = active && sprp2(n, q);
+    const bool pass = active && prp_test(n, q);
     const u32 ballot = __ballot_sync(0xffffffffu, pass);
     if (ballot == 0) return;
     const int lane = threadIdx.x & 31;
@@ -261,8 +261,8 @@ __global__ void __launch_bounds__(kTestThreads) k_test_prps(u32 *primecount, con
         const u64 p = prime[i];
         const u64 q = inv ? inv[i] : inv64(p);
         const D2 one = m2_one(p);
-        const D2 s = wieferich_digits(p, q, one);
-        const D2 c = wss_digits(p, q, one);
+        D2 s, c;
+        both_digits(p, q, one, s, c);
         sum += (s.d1 & 0xffffffffull) + (c.d1 & 0xffffffffull);
         int rem, quot, res;
         if (wieferich_classify(p, s, rem, quot)) emit_hit(hits, p, 1093, rem, quot);
@@ -278,8 +278,8 @@ __global__ void k_digits(const u64 *primes, u64 n, u64 *out) {
         const u64 p = primes[i];
         const u64 q = inv64(p);
         const D2 one = m2_one(p);
-        const D2 s = wieferich_digits(p, q, one);
-        const D2 c = wss_digits(p, q, one);
+        D2 s, c;
+        both_digits(p, q, one, s, c);
         out[4 * i] = s.d0;
         out[4 * i + 1] = s.d1;
         out[4 * i + 2] = c.d0;

@@ -1,0 +1,174 @@
+// ww_tests.cuh -- the Wieferich and Wall-Sun-Sun tests of one prime, and the
+// reference's hit classification.
+//
+// The mod p^2 arithmetic is a policy: Arith64 uses 64-bit C products
+// (ww_arith.cuh), Arith32 the explicit 32-bit carry chains (ww_chain.cuh).
+// Both produce the same canonical digits; kernels and the host self-test
+// use WW_ARITH (Arith32 unless WW_ARITH_VERSION is 1).
+#pragma once
+
+#include "ww_arith.cuh"
+#include "ww_chain.cuh"
+
+namespace ww {
+
+struct Arith64 {
+    u64 p, q;
+    WW_HD Arith64(u64 p_, u64 q_) : p(p_), q(q_) {}
+    WW_HD D2 mul(D2 x, D2 y) const { return m2_mul(x, y, p, q); }
+    WW_HD D2 sqr(D2 x) const { return m2_sqr(x, p, q); }
+    WW_HD D2 redc(D2 x) const { return m2_redc(x, p, q); }
+};
+
+struct Arith32 {
+    P32 P;
+    WW_HD Arith32(u64 p, u64 q) : P(make_p32(p, q)) {}
+    WW_HD D2 mul(D2 x, D2 y) const { return m2_mul32(x, y, P); }
+    WW_HD D2 sqr(D2 x) const { return m2_sqr32(x, P); }
+    WW_HD D2 redc(D2 x) const { return m2_redc32(x, P); }
+};
+
+#if defined(WW_ARITH_VERSION) && WW_ARITH_VERSION == 1
+typedef Arith64 WW_ARITH;
+WW_HD bool prp_test(u64 n, u64 &q) { return sprp2(n, q); }
+#else
+typedef Arith32 WW_ARITH;
+WW_HD bool prp_test(u64 n, u64 &q) { return sprp2_32(n, q); }
+#endif
+
+WW_HD int top_bit(u64 x) {
+#if defined(__CUDA_ARCH__)
+    return 63 - __clzll((long long)x);
+#else
+    return 63 - __builtin_clzll(x);
+#endif
+}
+
+WW_HD D2 sel(bool c, D2 a, D2 b) {
+    D2 r;
+    r.d0 = c ? a.d0 : b.d0;
+    r.d1 = c ? a.d1 : b.d1;
+    return r;
+}
+
+// 2^((p-1)/2) mod p^2 as canonical digits: left-to-right powering of 2, a
+// squaring per exponent bit and a doubling where the bit is set
+// (wieferich.cl:219-245).
+template <class A>
+WW_HD D2 wieferich_digits_t(u64 p, u64 q, D2 one) {
+    const A ar(p, q);
+    const u64 e = p >> 1;
+    D2 a = m2_dbl(one, p);
+    for (int i = top_bit(e) - 1; i >= 0; --i) {
+        a = ar.sqr(a);
+        a = sel((e >> i) & 1, m2_dbl(a, p), a);
+    }
+    return ar.redc(a);
+}
+
+// F_{p-(p|5)} mod p^2 as canonical digits.  The reference walks the
+// (F_k, F_{k-1}) doubling ladder, two squarings and a product per bit
+// (wallsunsun.cl:242-300).  Here the Lucas numbers V_k = L_k run a
+// Montgomery ladder (V_k, V_{k+1}), one squaring and one product per bit:
+//   V_2k = V_k^2 - 2(-1)^k,  V_2k+1 = V_k V_k+1 - (-1)^k,
+//   V_2k+2 = V_k+1^2 + 2(-1)^k,
+// and F_n = (2 V_{n+1} - V_n) / 5 gives the same residue exactly (5 is a
+// unit mod p^2 since p has no factor below 127).
+template <class A>
+WW_HD D2 wss_digits_t(u64 p, u64 q, D2 one) {
+    const A ar(p, q);
+    const u32 pm5 = (u32)(p % 5);
+    const u64 n = (pm5 == 2 || pm5 == 3) ? p + 1 : p - 1;  // p - (p|5)
+    const D2 zero = {0, 0};
+    const D2 two = m2_dbl(one, p);
+    const D2 mone = m2_sub(zero, one, p);
+    const D2 mtwo = m2_sub(zero, two, p);
+    D2 a = one;                  // V_1
+    D2 b = m2_add(two, one, p);  // V_2
+    bool odd = true;             // parity of the ladder index k
+    for (int i = top_bit(n) - 1; i >= 0; --i) {
+        const bool bit = (n >> i) & 1;
+        const D2 sq = ar.sqr(sel(bit, b, a));
+        const D2 pr = ar.mul(a, b);
+        const D2 np = m2_add(pr, sel(odd, one, mone), p);             // V_k V_k+1 - (-1)^k
+        const D2 ns = m2_add(sq, sel(bit ^ odd, two, mtwo), p);       // V^2 -/+ 2(-1)^k
+        a = sel(bit, np, ns);
+        b = sel(bit, ns, np);
+        odd = bit;
+    }
+    const D2 t = ar.redc(m2_sub(m2_dbl(b, p), a, p));
+    return m2_div5(t, p);
+}
+
+// Both tests in one loop: each iteration advances the Lucas ladder by one
+// bit of p - (p|5) and the Wieferich powering by one bit of (p-1)/2, so the
+// three products of an iteration are independent and overlap in the pipe.
+// The Lucas exponent is one or two bits longer; its first steps run alone.
+template <class A>
+WW_HD void both_digits_t(u64 p, u64 q, D2 one, D2 &s_out, D2 &c_out) {
+    const A ar(p, q);
+    const u32 pm5 = (u32)(p % 5);
+    const u64 n = (pm5 == 2 || pm5 == 3) ? p + 1 : p - 1;
+    const u64 e = p >> 1;
+    const int top_e = top_bit(e);
+    const D2 zero = {0, 0};
+    const D2 two = m2_dbl(one, p);
+    const D2 mone = m2_sub(zero, one, p);
+    const D2 mtwo = m2_sub(zero, two, p);
+    D2 a = one, b = m2_add(two, one, p);
+    D2 w = two;
+    bool odd = true;
+    for (int i = top_bit(n) - 1; i >= 0; --i) {
+        const bool bit = (n >> i) & 1;
+        const D2 sq = ar.sqr(sel(bit, b, a));
+        const D2 pr = ar.mul(a, b);
+        if (i < top_e) {
+            w = ar.sqr(w);
+            w = sel((e >> i) & 1, m2_dbl(w, p), w);
+        }
+        const D2 np = m2_add(pr, sel(odd, one, mone), p);
+        const D2 ns = m2_add(sq, sel(bit ^ odd, two, mtwo), p);
+        a = sel(bit, np, ns);
+        b = sel(bit, ns, np);
+        odd = bit;
+    }
+    s_out = ar.redc(w);
+    c_out = m2_div5(ar.redc(m2_sub(m2_dbl(b, p), a, p)), p);
+}
+
+WW_HD D2 wieferich_digits(u64 p, u64 q, D2 one) { return wieferich_digits_t<WW_ARITH>(p, q, one); }
+WW_HD void both_digits(u64 p, u64 q, D2 one, D2 &s, D2 &c) { both_digits_t<WW_ARITH>(p, q, one, s, c); }
+WW_HD D2 wss_digits(u64 p, u64 q, D2 one) { return wss_digits_t<WW_ARITH>(p, q, one); }
+
+// ------------------------------------------------------------ classification
+
+constexpr u64 kThreshold = 1000;  // WW.h:8 SPECIAL_THRESHOLD
+
+// wieferich.cl:248-293.  Returns true and fills rem/quot for a hit.
+WW_HD bool wieferich_classify(u64 p, D2 s, int &rem, int &quot) {
+    if (((s.d1 == 0) & (s.d0 == 1)) | ((s.d1 == p - 1) & (s.d0 == p - 1))) {
+        rem = 1;
+        quot = 0;
+        return true;
+    }
+    if (s.d1 <= kThreshold) {
+        if (s.d0 == 1) { rem = 1; quot = (int)s.d1; return true; }
+        if (s.d0 == p - 1) { rem = -1; quot = (int)(s.d1 + 1); return true; }
+        return false;
+    }
+    if (s.d1 >= p - kThreshold) {
+        if (s.d0 == 1) { rem = 1; quot = (int)(s.d1 - p); return true; }
+        if (s.d0 == p - 1) { rem = -1; quot = (int)(s.d1 + 1 - p); return true; }
+    }
+    return false;
+}
+
+// wallsunsun.cl:325-349.  result 1 = WSS prime, 2 = special instance.
+WW_HD bool wss_classify(u64 p, D2 c, int &result, int &quot) {
+    if (c.d1 == 0) { result = 1; quot = 0; return true; }
+    if (c.d1 <= kThreshold) { result = 2; quot = (int)c.d1; return true; }
+    if (c.d1 >= p - kThreshold) { result = 2; quot = (int)(c.d1 - p); return true; }
+    return false;
+}
+
+}  // namespace ww

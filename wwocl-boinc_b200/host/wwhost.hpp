@@ -1,0 +1,147 @@
+// wwhost.hpp -- host services of the wwocl program: A/B checkpoint files,
+// the results file, the CPU prime list used to check the GPU PRP list, and
+// a monotonic clock.  Behaviour follows the reference's main.cpp; every
+// function cites the lines it mirrors.
+#pragma once
+
+#include <inttypes.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <chrono>
+#include <string>
+#include <vector>
+
+#include "wwcuda.h"
+
+namespace wwhost {
+
+struct Files {
+    std::string results = "results-WW.txt";  // main.cpp:40
+    std::string state_a = "stateA-WW.txt";   // main.cpp:41
+    std::string state_b = "stateB-WW.txt";   // main.cpp:42
+};
+
+struct State {
+    uint64_t current = 0, cksm = 0;
+    double psum = 0.0;
+    int pcnt = 0;
+};
+
+// write_state (main.cpp:103-130): write the file due next; switch to the
+// other one only when the close succeeded, so a torn write leaves the older
+// file intact.
+inline void write_state(const Files &f, uint64_t start, uint64_t stop, const State &s, bool &write_a_next) {
+    const std::string &name = write_a_next ? f.state_a : f.state_b;
+    FILE *out = fopen(name.c_str(), "w");
+    if (!out) {
+        fprintf(stderr, "Cannot open %s !!!\n", name.c_str());
+        return;
+    }
+    if (fprintf(out, "%" PRIu64 " %" PRIu64 " %" PRIu64 " %" PRIu64 " %lf %d\n", start, stop, s.current, s.cksm,
+                s.psum, s.pcnt) < 0) {
+        fprintf(stderr, "Cannot write to %s !!! Continuing...\n", name.c_str());
+        fclose(out);
+        return;
+    }
+    fflush(out);
+    fsync(fileno(out));
+    if (fclose(out) == 0) write_a_next = !write_a_next;
+}
+
+inline bool read_one(const std::string &name, uint64_t start, uint64_t stop, State &s) {
+    FILE *in = fopen(name.c_str(), "r");
+    if (!in) return false;
+    uint64_t a = 0, b = 0;
+    State t;
+    const int n = fscanf(in, "%" SCNu64 " %" SCNu64 " %" SCNu64 " %" SCNu64 " %lf %d", &a, &b, &t.current, &t.cksm,
+                         &t.psum, &t.pcnt);
+    fclose(in);
+    if (n != 6) {
+        fprintf(stderr, "Cannot parse %s !!!\n", name.c_str());
+        return false;
+    }
+    if (a != start || b != stop) return false;  // main.cpp:157,173
+    s = t;
+    return true;
+}
+
+// read_state (main.cpp:136-209): the newer valid file wins (larger current;
+// B on a tie, as the reference's `current_a > current_b` test gives).
+inline bool read_state(const Files &f, uint64_t start, uint64_t stop, State &s, bool &write_a_next) {
+    State a, b;
+    bool ga = read_one(f.state_a, start, stop, a);
+    bool gb = read_one(f.state_b, start, stop, b);
+    if (ga && gb) {
+        if (a.current > b.current) gb = false;
+        else ga = false;
+    }
+    if (ga) {
+        s = a;
+        write_a_next = false;
+        return true;
+    }
+    if (gb) {
+        s = b;
+        write_a_next = true;
+        return true;
+    }
+    return false;
+}
+
+// report_solution (main.cpp:741-765): append and fsync.  Returns false on
+// failure (the caller exits, as the reference does).
+inline bool report_solution(const Files &f, const std::string &text) {
+    FILE *r = fopen(f.results.c_str(), "a");
+    if (!r) {
+        fprintf(stderr, "Cannot open %s !!!\n", f.results.c_str());
+        return false;
+    }
+    if (fprintf(r, "%s", text.c_str()) < 0) {
+        fprintf(stderr, "Cannot write to %s !!!\n", f.results.c_str());
+        fclose(r);
+        return false;
+    }
+    fflush(r);
+    fsync(fileno(r));
+    fclose(r);
+    return true;
+}
+
+inline bool truncate_results(const Files &f) {
+    FILE *r = fopen(f.results.c_str(), "w");  // main.cpp:1535-1540
+    if (!r) return false;
+    fclose(r);
+    return true;
+}
+
+// The primes of [lo, hi) for lo >= 127, the list primesieve produced in the
+// reference's PRP check (main.cpp:498): numbers with no prime factor <= 113
+// that pass the deterministic Miller-Rabin test.
+inline std::vector<uint64_t> cpu_primes(uint64_t lo, uint64_t hi) {
+    static const uint32_t small[29] = {3,  5,  7,  11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53,
+                                       59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113};
+    std::vector<uint64_t> out;
+    for (uint64_t n = lo | 1; n < hi && n >= lo; n += 2) {
+        bool sf = false;
+        for (uint32_t r : small)
+            if (n % r == 0) {
+                sf = true;
+                break;
+            }
+        if (!sf && ww_is_prime(n)) out.push_back(n);
+        if (n > UINT64_MAX - 2) break;
+    }
+    return out;
+}
+
+inline double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace wwhost

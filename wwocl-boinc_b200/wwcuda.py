@@ -94,6 +94,7 @@ _SIGS = {
     "ww_selftest_digits": (C.c_int, [_U64P, C.c_uint64, _U64P]),
     "ww_selftest_range": (C.c_int, [C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64),
                                     C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
+    "ww_selftest_m2": (C.c_int, [C.c_int, C.c_uint64, _U64P, C.c_uint64, _U64P]),
     "ww_random_primes": (C.c_int, [C.c_int, C.c_uint64, C.c_uint64, _U64P, C.POINTER(C.c_uint64)]),
     "ww_pipe_bench": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
@@ -161,6 +162,14 @@ def selftest_range(lo: int, hi: int) -> dict:
     a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint32()
     check(_L.ww_selftest_range(lo, hi, C.byref(a), C.byref(b), C.byref(c)), "ww_selftest_range")
     return dict(prp_count=a.value, checksum=b.value, result_count=c.value)
+
+
+def selftest_m2(op: int, p: int, xy: np.ndarray) -> np.ndarray:
+    xy = np.ascontiguousarray(xy, dtype=np.uint64).reshape(-1)
+    n = xy.size // 4
+    out = np.zeros(2 * n, dtype=np.uint64)
+    check(_L.ww_selftest_m2(op, p, xy, n, out), "ww_selftest_m2")
+    return out.reshape(-1, 2)
 
 
 def random_primes(seed: int, n: int, device: int = 0) -> tuple[np.ndarray, int]:
@@ -295,7 +304,7 @@ class Context:
             start = stop
         self.sync()
         c = self.counters()
-        c["hits"] = self.hits()
+        c["hits"] = [] if c["overflow"] & 2 else self.hits()
         return c
 
 
