@@ -47,6 +47,10 @@ def parse_args():
     ap.add_argument("--cpu-sample", type=int, default=1 << 20,
                     help="primes in the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-units", type=int, default=128,
+                    help="units of the uneven mix for the batched-vs-plain line (0: skip)")
+    ap.add_argument("--serve-seconds", type=float, default=10.0,
+                    help="length of the Poisson request stream (0: skip)")
     return ap.parse_args()
 
 
@@ -177,6 +181,99 @@ def run_reference(args):
     return 0
 
 
+def run_batched_vs_plain(ww, local: int, n_units: int, tune_units: int = 32):
+    """Config 4 subsample: the first n_units of the seed-11 uneven mix (widths
+    log-uniform in [1e6, 1e10], starts uniform in [1e15, 2^64-1e10], multiples
+    of 30).  Plain = one range per launch sequence (clear, sieve, test, read)
+    through the context API; batched = one persistent CUDA-graph launch over
+    the tile queue after the autotuner picked the configuration.  Per-unit
+    checksums and PRP counts must agree."""
+    units = ww.uneven_units(11, 4096)[:n_units]
+    ctx = ww.Context(local, max_prps=1 << 24, max_hits=15000)
+    b = ww.Batch(ctx)
+    cfg, _ = b.tune(units[:tune_units])
+    b.run(units)  # warm
+    ctx.marker(0)
+    res = b.run(units)
+    ctx.marker(1)
+    ctx.sync()
+    batch_ms = ctx.elapsed_ms(0, 1)
+    prps = sum(r["prp_count"] for r in res)
+    t0 = time.perf_counter()
+    alone = [ctx.run_range(a, z) for a, z in units]
+    plain_s = time.perf_counter() - t0
+    equal = all(r["checksum"] == a["checksum"] and r["prp_count"] == a["total_prp_count"] and
+                r["hits"] == a["result_count"] for r, a in zip(res, alone))
+    ctx.close()
+    numbers = sum(z - a for a, z in units)
+    return {"workload": f"first {n_units} units of the seed-11 uneven mix (config 4)", "units": n_units,
+            "numbers": numbers, "prps": prps, "batched_primes_per_s": prps / (batch_ms * 1e-3),
+            "plain_primes_per_s": prps / plain_s, "batched_numbers_per_s": numbers / (batch_ms * 1e-3),
+            "speedup_batched_vs_plain": plain_s / (batch_ms * 1e-3), "per_unit_bit_identical": bool(equal),
+            "tuned_config": {"seg_words": cfg[0], "seg_bytes": 4 * cfg[0], "threads": cfg[1],
+                             "primes_per_thread": cfg[2]}}
+
+
+def run_serving(ww, local: int, seconds: float, rate: float = 200.0, seed: int = 13, check_cpu: int = 12):
+    """Config 5, shortened: Poisson arrivals at `rate` req/s for `seconds`,
+    widths log-uniform in [1e5, 1e9], starts uniform in [1e12, 2^64-1e9].
+    Latency = completion time - arrival time on the host monotonic clock."""
+    rng = np.random.default_rng(seed)
+    arrivals, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > seconds:
+            break
+        arrivals.append(t)
+    widths = np.exp(rng.uniform(np.log(1e5), np.log(1e9), len(arrivals)))
+    starts = rng.integers(10**12, 2**64 - 10**9, len(arrivals), dtype=np.uint64)
+    reqs = [(i, int(s), int(s) + int(w)) for i, (s, w) in enumerate(zip(starts, widths))]
+    ctx = ww.Context(local, max_prps=1 << 20, max_hits=15000)
+    srv = ww.Server(ctx, prp_pool_bytes=24 << 30, max_active=256, epoch_tiles=1024, store_prps=True)
+    srv.submit([(10**9, 10**12, 10**12 + 10**6)])  # warm-up request
+    srv.drain()
+    done = {}
+    i = 0
+    t0 = time.monotonic()
+    while len(done) < len(reqs):
+        now = time.monotonic() - t0
+        batch = []
+        while i < len(reqs) and arrivals[i] <= now:
+            batch.append(reqs[i])
+            i += 1
+        if batch:
+            srv.submit(batch)
+        q, a, _ = srv.status()
+        if q == 0 and a == 0:
+            if i < len(reqs):
+                time.sleep(max(0.0, min(arrivals[i] - now, 0.01)))
+            continue
+        for r in srv.step():
+            done[r["id"]] = r
+    wall = time.monotonic() - t0
+    lat = np.array([done[k]["t_done"] - (t0 + arrivals[k]) for k in range(len(reqs))]) * 1e3
+    prps = sum(r["prp_count"] for r in done.values())
+    numbers = sum(b - a for _, a, b in reqs)
+    ok_status = all(r["status"] == 0 for r in done.values())
+    cpu_equal = None
+    try:
+        from oracle.oracle import RefCPU
+
+        if RefCPU.available():
+            ref = RefCPU()
+            small = sorted(reqs, key=lambda r: r[2] - r[1])[:check_cpu]
+            cpu_equal = all(ref.scan_range(a, b)["checksum"] == done[k]["checksum"] for k, a, b in small)
+    except OSError:
+        cpu_equal = None
+    srv.close()
+    ctx.close()
+    return {"workload": f"Poisson {rate:g} req/s for {seconds:g} s (config 5, seed 13), widths 1e5..1e9",
+            "requests": len(reqs), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "max_ms": float(lat.max()), "primes_per_s": prps / wall, "numbers_per_s": numbers / wall,
+            "offered_numbers_per_s": numbers / seconds, "all_ok": bool(ok_status),
+            "cpu_checksum_equal_on_smallest": cpu_equal}
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -298,10 +395,16 @@ def main():
         except (FileNotFoundError, OSError) as e:
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 
+    extra = {}
+    if args.batch_units:
+        extra["batched_vs_plain"] = run_batched_vs_plain(ww, local, args.batch_units)
+    if args.serve_seconds:
+        extra["serving"] = run_serving(ww, local, args.serve_seconds)
+
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": config(args, world),
+            "config": config(args, world), **extra,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
                     "d2h_bytes_per_step": 32 + hit_bytes * hits_per_step},
             "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu,

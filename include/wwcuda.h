@@ -187,6 +187,91 @@ typedef struct {
 int ww_get_buffers(ww_ctx *ctx, ww_buffers *out);
 
 /* ---------------------------------------------------------------------------
+ * Batched search (no reference counterpart; replaces running the reference
+ * program once per range).  Many ranges of uneven width run in one
+ * persistent, CUDA-graph-captured launch: the kernel pulls (range, segment)
+ * tiles from a device queue and runs sieve, PRP test and both tests on each
+ * tile inside one CTA.  Per-unit checksums equal those of running each
+ * range alone.  Hits carry the unit index.
+ * ------------------------------------------------------------------------- */
+
+typedef struct {
+    uint64_t start, end; /* [start, end), 127 <= start, or start == end */
+} ww_unit;
+
+typedef struct {
+    uint64_t checksum;  /* sum of both checksum terms over the unit's PRPs */
+    uint64_t prp_count; /* PRPs tested */
+    uint32_t hits;      /* hit records of the unit */
+    uint32_t tiles_done;
+} ww_unit_result;
+
+/* seg_words: 32-bit words of a tile's bitmap (64 integers per word);
+ * threads: per CTA; ppt: primes per thread in the test phase. */
+typedef struct {
+    uint32_t seg_words, threads, ppt, reserved;
+} ww_batch_cfg;
+
+int ww_batch_configs(ww_batch_cfg *out, uint32_t cap, uint32_t *n);
+int ww_batch_set_config(ww_ctx *ctx, const ww_batch_cfg *cfg);
+int ww_batch_get_config(ww_ctx *ctx, ww_batch_cfg *cfg);
+int ww_batch_reserve_hits(ww_ctx *ctx, uint32_t max_hits);
+/* Queue the units (async on the context stream); collect waits and reads
+ * the per-unit results. */
+int ww_batch_submit(ww_ctx *ctx, const ww_unit *units, uint32_t n);
+int ww_batch_collect(ww_ctx *ctx, ww_unit_result *out, uint32_t n, uint32_t *hit_count);
+int ww_batch_run(ww_ctx *ctx, const ww_unit *units, uint32_t n, ww_unit_result *out);
+int ww_batch_hits(ww_ctx *ctx, ww_hit *out, uint32_t *unit_of_hit, uint32_t cap, uint32_t *n);
+/* Autotuner (replaces profileGPU, main.cpp:959-1107): times every compiled
+ * configuration on the sample and keeps the fastest in the context. */
+int ww_batch_tune(ww_ctx *ctx, const ww_unit *sample, uint32_t n, ww_batch_cfg *best, float *best_ms);
+
+/* ---------------------------------------------------------------------------
+ * Request server (no reference counterpart; the reference runs one range
+ * per process).  Continuous batching: requests wait in a host queue and are
+ * admitted into device slots while slots and PRP-buffer memory last (each
+ * request reserves ww_prp_count_bound(start, end) * 8 bytes); every
+ * ww_server_step runs one bounded launch of the tile engine over all
+ * admitted requests (round-robin, each request's sieve cursor, checksum,
+ * counters and PRP buffer resident on the device) and returns the requests
+ * that finished.  A request's results equal those of running it alone.
+ * ------------------------------------------------------------------------- */
+
+typedef struct {
+    uint64_t id, start, end; /* [start, end), 127 <= start */
+} ww_request;
+
+typedef struct {
+    uint64_t id;
+    uint64_t checksum, prp_count;
+    uint64_t prps_stored;   /* PRPs written to the request's buffer */
+    uint32_t hits;          /* hit records (read them with ww_server_hits) */
+    int32_t status;         /* WW_OK, or WW_ERR_PRP_OVERFLOW / WW_ERR_HIT_OVERFLOW */
+    double t_submit, t_admit, t_done; /* host monotonic seconds */
+} ww_request_result;
+
+typedef struct {
+    uint64_t prp_pool_bytes; /* device memory for per-request PRP buffers */
+    uint32_t max_active;     /* device slots */
+    uint32_t epoch_tiles;    /* most tiles one step launches */
+    uint32_t max_hits;       /* hit records per step */
+    uint32_t store_prps;     /* 1: keep each request's PRP list on the device */
+} ww_server_cfg;
+
+int ww_server_open(ww_ctx *ctx, const ww_server_cfg *cfg);
+int ww_server_close(ww_ctx *ctx);
+int ww_server_submit(ww_ctx *ctx, const ww_request *reqs, uint32_t n);
+/* Admit, run one epoch, collect finished requests into done[0..*ndone). */
+int ww_server_step(ww_ctx *ctx, ww_request_result *done, uint32_t cap, uint32_t *ndone);
+int ww_server_status(ww_ctx *ctx, uint32_t *queued, uint32_t *active, uint64_t *pool_used);
+/* Hits of a finished request (kept until the next ww_server_hits call for
+ * that id). */
+int ww_server_hits(ww_ctx *ctx, uint64_t id, ww_hit *out, uint32_t cap, uint32_t *n);
+/* PRP list of a finished request with store_prps (read before its slot is
+ * reused: valid until the next ww_server_step). */
+int ww_server_prps(ww_ctx *ctx, uint64_t id, uint64_t *out, uint64_t cap, uint64_t *n);
+
+/* ---------------------------------------------------------------------------
  * 3. Host helpers of the reference program (main.cpp), exported so every
  *    caller shares one implementation.
  * ------------------------------------------------------------------------- */
@@ -220,10 +305,17 @@ int ww_selftest_digits(const uint64_t *primes, uint64_t n, uint64_t *out);
 int ww_selftest_range(uint64_t lo, uint64_t hi, uint64_t *prp_count, uint64_t *checksum,
                       uint32_t *result_count);
 /* One operation of the kernels' mod p^2 arithmetic on the host, for
- * checking it operand by operand: op 0 = X*Y/2^64, 1 = X^2/2^64,
- * 2 = X/2^64 (mod p^2), inputs and outputs as digit pairs x0 + p x1;
- * xy = (x0, x1, y0, y1) per case, out = (z0, z1). */
+ * checking it operand by operand: op & 15 = 0 X*Y/2^64, 1 X^2/2^64,
+ * 2 X/2^64 (mod p^2); op >> 4 picks the formulation (0 the kernels' own,
+ * 1 64-bit products, 2 PTX carry chains, 3 wide 32x32+64 products).
+ * Inputs and outputs are digit pairs x0 + p x1; xy = (x0, x1, y0, y1) per
+ * case, out = (z0, z1). */
 int ww_selftest_m2(int op, uint64_t p, const uint64_t *xy, uint64_t n, uint64_t *out);
+/* The kernels' PRP-test candidates of [lo, hi) computed on the host
+ * (small primes 3..113, then the deep sieve to 2^16 with its rescue list of
+ * possible base-2 pseudoprimes), sorted; *rescued = rescue-list length. */
+int ww_selftest_candidates(uint64_t lo, uint64_t hi, uint64_t *out, uint64_t cap, uint64_t *n,
+                           uint64_t *rescued);
 
 /* ---------------------------------------------------------------------------
  * 4. Measurement utilities (no reference counterpart).

@@ -52,6 +52,7 @@ class Oracle:
         L = C.CDLL(str(path))
         self.L = L
         L.wo_sprp2.argtypes = [C.c_uint64]
+        L.wo_small_factor.argtypes = [C.c_uint64]
         L.wo_is_prp.argtypes = [C.c_uint64]
         L.wo_is_prime.argtypes = [C.c_uint64]
         L.wo_inv64.argtypes = [C.c_uint64]
@@ -77,6 +78,9 @@ class Oracle:
     # scalar helpers -----------------------------------------------------
     def sprp2(self, n: int) -> bool:
         return bool(self.L.wo_sprp2(n))
+
+    def small_factor(self, n: int) -> bool:
+        return bool(self.L.wo_small_factor(n))
 
     def is_prp(self, n: int) -> bool:
         return bool(self.L.wo_is_prp(n))

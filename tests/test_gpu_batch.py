@@ -1,0 +1,72 @@
+"""The batched persistent search: per-unit checksums, PRP counts and hits
+bit-identical to running each unit alone, for every compiled configuration,
+and against the oracle on small units."""
+from __future__ import annotations
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(ww):
+    c = ww.Context(0, max_prps=1 << 22, max_hits=15000)
+    yield c
+    c.close()
+
+
+def _alone(ctx, lo, hi):
+    r = ctx.run_range(lo, hi)
+    return r["checksum"], r["total_prp_count"], r["result_count"]
+
+
+def test_small_units_match_oracle(ww, ctx, oracle):
+    units = [(127, 1_000_000), (4_294_000_000, 4_295_500_000), (2**64 - 2**35, 2**64 - 2**35 + 700_001),
+             (2276306935816523 - 5000, 2276306935816523 + 5000), (1000, 1000), (2**64 - 1_000_001, 2**64 - 1)]
+    b = ww.Batch(ctx)
+    got = b.run(units)
+    hits = b.hits()
+    for i, (lo, hi) in enumerate(units):
+        if hi > lo:
+            want, _, whits = oracle.scan_range(lo, hi, hit_cap=100000)
+        else:
+            want, whits = dict(checksum=0, prp_count=0, gpu_results=0), []
+        assert got[i]["checksum"] == want["checksum"], i
+        assert got[i]["prp_count"] == want["prp_count"], i
+        assert got[i]["hits"] == want["gpu_results"], i
+        assert sorted(h[1:] for h in hits if h[0] == i) == sorted(whits), i
+
+
+def test_every_config_matches_alone(ww, ctx):
+    units = ww.uneven_units(11, 24, wmin=1e5, wmax=3e8)
+    alone = [_alone(ctx, lo, hi) for lo, hi in units]
+    b = ww.Batch(ctx)
+    for cfg in ww.batch_configs():
+        b.set_config(*cfg)
+        got = b.run(units)
+        for i, r in enumerate(got):
+            assert (r["checksum"], r["prp_count"], r["hits"]) == alone[i], (cfg, i)
+
+
+def test_tuner_picks_a_config(ww, ctx):
+    b = ww.Batch(ctx)
+    sample = ww.uneven_units(11, 64, wmin=1e6, wmax=1e9)
+    cfg, ms = b.tune(sample)
+    assert cfg in ww.batch_configs() and ms > 0
+    assert b.config() == cfg
+
+
+def test_config4_subsample_matches_alone(ww, ctx):
+    """First 48 units of the seed-11 uneven mix (widths 1e6..1e10), batched
+    versus one range per launch."""
+    units = ww.uneven_units(11, 4096)[:48]
+    b = ww.Batch(ctx)
+    got = b.run(units)
+    for i, (lo, hi) in enumerate(units):
+        assert (got[i]["checksum"], got[i]["prp_count"], got[i]["hits"]) == _alone(ctx, lo, hi), i
+
+
+def test_bad_unit_is_rejected(ww, ctx):
+    b = ww.Batch(ctx)
+    with pytest.raises(ww.WWError):
+        b.run([(100, 1000)])

@@ -1,0 +1,86 @@
+"""The request server: continuous batching keeps every request's result
+(checksum, PRP count, hits, PRP list) identical to running it alone, and
+admission respects the PRP-buffer memory budget."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(ww):
+    c = ww.Context(0, max_prps=1 << 22, max_hits=15000)
+    yield c
+    c.close()
+
+
+def _requests(ww, n, seed=13):
+    units = ww.uneven_units(seed, n, wmin=1e5, wmax=3e7, smin=10**12, smax=2**64 - 10**9)
+    return [(1000 + i, a, b) for i, (a, b) in enumerate(units)]
+
+
+def test_mix_equals_alone(ww, ctx):
+    reqs = _requests(ww, 40)
+    srv = ww.Server(ctx, prp_pool_bytes=1 << 30, max_active=16, epoch_tiles=64)
+    srv.submit(reqs)
+    mixed = {r["id"]: r for r in srv.drain()}
+    hits_mixed = {rid: sorted(srv.hits(rid)) for rid, _, _ in reqs}
+    srv.close()
+    assert set(mixed) == {r[0] for r in reqs}
+    for rid, a, b in reqs:
+        srv1 = ww.Server(ctx, prp_pool_bytes=1 << 30, max_active=4, epoch_tiles=4096)
+        srv1.submit([(rid, a, b)])
+        alone = srv1.drain()
+        assert len(alone) == 1
+        al = alone[0]
+        assert (mixed[rid]["checksum"], mixed[rid]["prp_count"], mixed[rid]["hits"]) == \
+               (al["checksum"], al["prp_count"], al["hits"]), rid
+        assert sorted(srv1.hits(rid)) == hits_mixed[rid]
+        srv1.close()
+        ref = ctx.run_range(a, b)
+        assert (al["checksum"], al["prp_count"]) == (ref["checksum"], ref["total_prp_count"])
+
+
+def test_results_match_oracle_and_prp_lists(ww, ctx, oracle):
+    reqs = [(1, 2**64 - 2**35, 2**64 - 2**35 + 300_000), (2, 10**12, 10**12 + 400_000),
+            (3, 2276306935816523 - 7000, 2276306935816523 + 7000), (4, 127, 200_000)]
+    srv = ww.Server(ctx, prp_pool_bytes=1 << 26, max_active=8, epoch_tiles=16)
+    srv.submit(reqs)
+    got = {}
+    for _ in range(1000):
+        for r in srv.step():
+            got[r["id"]] = (r, srv.prps(r["id"], r["prps_stored"]))
+        q, a, _ = srv.status()
+        if q == 0 and a == 0:
+            break
+    for rid, a, b in reqs:
+        r, prps = got[rid]
+        want, wprps, whits = oracle.scan_range(a, b, want_prps=True, prp_cap=(b - a) // 2 + 8, hit_cap=10000)
+        assert r["status"] == 0
+        assert (r["checksum"], r["prp_count"], r["hits"]) == (want["checksum"], want["prp_count"],
+                                                             want["gpu_results"])
+        assert np.array_equal(np.sort(prps), wprps)
+        assert sorted(srv.hits(rid)) == sorted(whits)
+    srv.close()
+
+
+def test_admission_waits_for_memory(ww, ctx):
+    # each request reserves ww_prp_count_bound * 8 bytes; a pool for about one
+    # request at a time forces one-at-a-time admission and still finishes
+    reqs = _requests(ww, 6, seed=5)
+    need = max(ww.prp_count_bound(a, b) for _, a, b in reqs) * 8
+    srv = ww.Server(ctx, prp_pool_bytes=need + 4096, max_active=8, epoch_tiles=32)
+    srv.submit(reqs)
+    seen_active = 0
+    done = []
+    for _ in range(100000):
+        done += srv.step()
+        q, a, used = srv.status()
+        seen_active = max(seen_active, a)
+        assert used <= need + 4096
+        if q == 0 and a == 0:
+            break
+    assert len(done) == len(reqs) and seen_active <= 2
+    srv.close()

@@ -140,9 +140,10 @@ def test_m2_arithmetic_edge_cases(ww):
         cases = [(a, b, c, d) for a in special for b in special[:6] for c in special[:6] for d in special]
         xy = np.array(cases, dtype=np.uint64)
         for op in (0, 1, 2):
-            got = ww.selftest_m2(op, p, xy)
             want = [_m2_exact(op, p, *c) for c in cases]
-            assert [tuple(map(int, g)) for g in got] == want, (p, op)
+            for impl in (0, 1, 2, 3):
+                got = ww.selftest_m2(op | impl << 4, p, xy)
+                assert [tuple(map(int, g)) for g in got] == want, (p, op, impl)
 
 
 def test_m2_arithmetic_random(ww):
@@ -152,6 +153,36 @@ def test_m2_arithmetic_random(ww):
         cases = [tuple(int(v) % p for v in rng.integers(0, 2**64 - 1, 4, dtype=np.uint64)) for _ in range(500)]
         xy = np.array(cases, dtype=np.uint64)
         for op in (0, 1, 2):
-            got = ww.selftest_m2(op, p, xy)
             want = [_m2_exact(op, p, *c) for c in cases]
-            assert [tuple(map(int, g)) for g in got] == want, (p, op)
+            for impl in (0, 1, 2, 3):
+                got = ww.selftest_m2(op | impl << 4, p, xy)
+                assert [tuple(map(int, g)) for g in got] == want, (p, op, impl)
+
+
+@pytest.mark.parametrize("lo,hi", [(127, 2_000_000), (1_373_553, 4_373_653), (2**32 - 10**6, 2**32 + 10**6),
+                                   (2**64 - 2 * 10**6 - 1, 2**64 - 1), (10**15, 10**15 + 3_000_000)])
+def test_deep_sieve_keeps_every_prp(ww, oracle, lo, hi):
+    """The deep sieve (primes to 2^16) with its rescue list of possible
+    base-2 pseudoprimes keeps every PRP of the reference's definition, and
+    only numbers with no factor <= 113 reach the PRP test."""
+    cand, rescued = ww.selftest_candidates(lo, hi)
+    summ, prps, _ = oracle.scan_range(lo, hi, want_prps=True, prp_cap=(hi - lo) // 2 + 8)
+    assert np.all(np.isin(prps, cand)), "a PRP was sieved out"
+    assert not np.any(np.isin(cand, np.array([1], np.uint64)))
+    sample = cand[:: max(1, cand.size // 2000)]
+    assert all(not oracle.small_factor(int(x)) for x in sample)
+    # about 0.05 candidates per integer at large n (Mertens), against 0.119
+    # after 113; at small n the primes themselves are denser than that
+    assert cand.size < 0.062 * (hi - lo) + 1.1 * prps.size
+    spsp = [int(p) for p in prps if not oracle.is_prime(int(p))]
+    for n in spsp:
+        assert n in set(cand.tolist())
+
+
+def test_deep_sieve_rescues_pseudoprimes_with_deep_factors(ww, oracle):
+    # 49141 = 157 * 313 and 88357 = 149 * 593 are base-2 strong pseudoprimes
+    # whose factors are deep-sieve primes: only the rescue list keeps them
+    for n in (49141, 88357, 104653):
+        assert oracle.is_prp(n) and not oracle.is_prime(n)
+        cand, rescued = ww.selftest_candidates(n - 2000, n + 2000)
+        assert n in cand.tolist() and rescued >= 1

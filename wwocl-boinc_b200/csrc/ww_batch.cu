@@ -1,0 +1,753 @@
+// ww_batch.cu -- host side of the batched search (include/wwcuda.h section 5):
+// the compiled configurations, the tile table, the CUDA-graph-captured
+// persistent launch and the autotuner that picks segment size, threads per
+// CTA and primes per thread by timing them on a sample of the workload.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <deque>
+#include <map>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/wwcuda.h"
+#include "ww_batch.cuh"
+
+using namespace ww;
+
+namespace ww {
+void set_err(const char *fmt, ...);  // ww_capi.cu
+int ctx_device(ww_ctx *c);
+void *ctx_stream(ww_ctx *c);
+struct BatchState;
+BatchState *&ctx_batch(ww_ctx *c);
+}  // namespace ww
+
+namespace {
+
+#define WW_CU(call)                                                                             \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) {                                                                \
+            set_err("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return WW_ERR_CUDA;                                                                 \
+        }                                                                                       \
+    } while (0)
+
+typedef void (*TileKernel)(BatchArgs);
+
+struct CfgEntry {
+    int seg_words, threads, ppt;
+    TileKernel kernel;        // static tile table (batch)
+    TileKernel serve_kernel;  // round-robin over request slots (serving)
+    size_t smem;
+};
+
+template <int W, int T, int P>
+CfgEntry entry() {
+    typedef BatchCfg<W, T, P> C;
+    return CfgEntry{W, T, P, &k_tiles<C, false>, &k_tiles<C, true>, batch_smem_bytes<C>()};
+}
+
+// Segment bitmaps of 16-128 KB (the whole segment must sit in one CTA's
+// shared memory, at most 227 KB), 128-1024 threads, 1-2 primes per thread.
+const std::vector<CfgEntry> &configs() {
+    static const std::vector<CfgEntry> table = {
+        entry<4096, 128, 1>(),   entry<4096, 256, 1>(),   entry<4096, 512, 1>(),   entry<4096, 256, 2>(),
+        entry<8192, 256, 1>(),   entry<8192, 512, 1>(),   entry<8192, 1024, 1>(),  entry<8192, 256, 2>(),
+        entry<16384, 256, 1>(),  entry<16384, 512, 1>(),  entry<16384, 1024, 1>(), entry<16384, 512, 2>(),
+        entry<32768, 512, 1>(),  entry<32768, 1024, 1>(),
+    };
+    return table;
+}
+
+const CfgEntry *find_cfg(const ww_batch_cfg &c) {
+    for (const CfgEntry &e : configs())
+        if (e.seg_words == (int)c.seg_words && e.threads == (int)c.threads && e.ppt == (int)c.ppt) return &e;
+    return nullptr;
+}
+
+ww_batch_cfg default_cfg() { return ww_batch_cfg{8192, 256, 1, 0}; }
+
+}  // namespace
+
+namespace ww {
+
+struct BatchState {
+    UnitState *d_units = nullptr;
+    u64 *d_first = nullptr;
+    u64 *d_next = nullptr;
+    u32 *d_rr = nullptr, *d_epoch = nullptr;
+    u32 *d_hit_count = nullptr, *d_overflow = nullptr, *d_hit_unit = nullptr;
+    u64 *d_hit_p = nullptr;
+    int *d_hit_res = nullptr, *d_hit_rem = nullptr, *d_hit_quot = nullptr;
+    u32 unit_cap = 0, hit_cap = 0;
+    UnitState *h_units = nullptr;  // pinned mirror of d_units
+    u64 *h_first = nullptr;        // pinned tile table
+    u32 n_units = 0;
+    cudaGraphExec_t exec = nullptr;
+    bool tuned = false;
+    ww_batch_cfg cfg = default_cfg();
+
+    ~BatchState() {
+        cudaFree(d_units);
+        cudaFree(d_first);
+        cudaFree(d_next);
+        cudaFree(d_rr);
+        cudaFree(d_epoch);
+        cudaFree(d_hit_count);
+        cudaFree(d_overflow);
+        cudaFree(d_hit_unit);
+        cudaFree(d_hit_p);
+        cudaFree(d_hit_res);
+        cudaFree(d_hit_rem);
+        cudaFree(d_hit_quot);
+        if (h_units) cudaFreeHost(h_units);
+        if (h_first) cudaFreeHost(h_first);
+        if (exec) cudaGraphExecDestroy(exec);
+    }
+};
+
+void destroy_batch_state(BatchState *s) { delete s; }
+
+}  // namespace ww
+
+namespace {
+
+int ensure_capacity(BatchState &b, u32 n_units, u32 hit_cap) {
+    if (n_units > b.unit_cap) {
+        cudaFree(b.d_units);
+        cudaFree(b.d_first);
+        if (b.h_units) cudaFreeHost(b.h_units);
+        if (b.h_first) cudaFreeHost(b.h_first);
+        b.d_units = nullptr;
+        b.d_first = nullptr;
+        b.h_units = nullptr;
+        b.h_first = nullptr;
+        b.unit_cap = 0;
+        WW_CU(cudaMalloc(&b.d_units, (size_t)n_units * sizeof(UnitState)));
+        WW_CU(cudaMalloc(&b.d_first, ((size_t)n_units + 1) * sizeof(u64)));
+        WW_CU(cudaMallocHost(&b.h_units, (size_t)n_units * sizeof(UnitState)));
+        WW_CU(cudaMallocHost(&b.h_first, ((size_t)n_units + 1) * sizeof(u64)));
+        b.unit_cap = n_units;
+    }
+    if (!b.d_next) {
+        WW_CU(cudaMalloc(&b.d_next, sizeof(u64)));
+        WW_CU(cudaMalloc(&b.d_rr, sizeof(u32)));
+        WW_CU(cudaMalloc(&b.d_epoch, sizeof(u32)));
+        WW_CU(cudaMalloc(&b.d_hit_count, sizeof(u32)));
+        WW_CU(cudaMalloc(&b.d_overflow, sizeof(u32)));
+    }
+    if (hit_cap > b.hit_cap) {
+        cudaFree(b.d_hit_unit);
+        cudaFree(b.d_hit_p);
+        cudaFree(b.d_hit_res);
+        cudaFree(b.d_hit_rem);
+        cudaFree(b.d_hit_quot);
+        b.hit_cap = 0;
+        WW_CU(cudaMalloc(&b.d_hit_unit, (size_t)hit_cap * 4));
+        WW_CU(cudaMalloc(&b.d_hit_p, (size_t)hit_cap * 8));
+        WW_CU(cudaMalloc(&b.d_hit_res, (size_t)hit_cap * 4));
+        WW_CU(cudaMalloc(&b.d_hit_rem, (size_t)hit_cap * 4));
+        WW_CU(cudaMalloc(&b.d_hit_quot, (size_t)hit_cap * 4));
+        b.hit_cap = hit_cap;
+    }
+    return WW_OK;
+}
+
+BatchArgs make_args(BatchState &b, u32 n, u64 n_tiles) {
+    BatchArgs a;
+    a.units = b.d_units;
+    a.n_units = n;
+    a.tile_first = b.d_first;
+    a.n_tiles = n_tiles;
+    a.next_tile = b.d_next;
+    a.rr = b.d_rr;
+    a.epoch_tiles = b.d_epoch;
+    a.budget = 0;
+    a.hit_p = b.d_hit_p;
+    a.hit_result = b.d_hit_res;
+    a.hit_rem = b.d_hit_rem;
+    a.hit_quot = b.d_hit_quot;
+    a.hit_unit = b.d_hit_unit;
+    a.hit_count = b.d_hit_count;
+    a.hit_capacity = b.hit_cap;
+    a.overflow = b.d_overflow;
+    return a;
+}
+
+int launch_grid(const CfgEntry &e, int device, int *grid) {
+    WW_CU(cudaFuncSetAttribute(e.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem));
+    int per_sm = 0, sms = 0;
+    WW_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, e.kernel, e.threads, e.smem));
+    WW_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    if (per_sm < 1) return set_err("batch config does not fit on an SM"), WW_ERR_ARG;
+    *grid = per_sm * sms;
+    return WW_OK;
+}
+
+// Upload the units (their device state doubles as the cleared result
+// block) and the tile table, then record clear + persistent launch as a
+// CUDA graph on the stream and run it.
+int run_batch(ww_ctx *ctx, BatchState &b, const ww_unit *units, uint32_t n, const CfgEntry &e,
+              u64 *n_tiles_out) {
+    const int dev = ctx_device(ctx);
+    cudaStream_t st = (cudaStream_t)ctx_stream(ctx);
+    const u64 tile = 64ull * (u64)e.seg_words;
+    int rc = ensure_capacity(b, n ? n : 1, b.hit_cap ? b.hit_cap : 1u << 16);
+    if (rc) return rc;
+    WW_CU(cudaStreamSynchronize(st));  // the pinned mirror may still feed a previous launch
+    u64 acc = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (units[i].end < units[i].start || (units[i].end > units[i].start && units[i].start < 127))
+            return set_err("unit %u: bad range [%llu, %llu)", i, (unsigned long long)units[i].start,
+                           (unsigned long long)units[i].end), WW_ERR_ARG;
+        UnitState &u = b.h_units[i];
+        memset(&u, 0, sizeof u);
+        u.start = units[i].start;
+        u.end = units[i].end;
+        const u64 w = units[i].end - units[i].start;
+        u.n_tiles = w / tile + (w % tile ? 1 : 0);
+        u.active = 1;
+        b.h_first[i] = acc;
+        acc += u.n_tiles;
+    }
+    b.h_first[n] = acc;
+    b.n_units = n;
+    *n_tiles_out = acc;
+    int grid = 0;
+    rc = launch_grid(e, dev, &grid);
+    if (rc) return rc;
+    const BatchArgs a = make_args(b, n, acc);
+
+    cudaGraph_t g = nullptr;
+    WW_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(b.d_units, b.h_units, (size_t)n * sizeof(UnitState), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(b.d_first, b.h_first, ((size_t)n + 1) * sizeof(u64), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(b.d_next, 0, sizeof(u64), st);
+    cudaMemsetAsync(b.d_hit_count, 0, sizeof(u32), st);
+    cudaMemsetAsync(b.d_overflow, 0, sizeof(u32), st);
+    if (acc) e.kernel<<<grid, e.threads, e.smem, st>>>(a);
+    cudaError_t ce = cudaStreamEndCapture(st, &g);
+    if (ce != cudaSuccess) return set_err("graph capture: %s", cudaGetErrorString(ce)), WW_ERR_CUDA;
+    bool updated = false;
+    if (b.exec) {
+        cudaGraphExecUpdateResultInfo info;
+        updated = cudaGraphExecUpdate(b.exec, g, &info) == cudaSuccess;
+        if (!updated) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(b.exec);
+            b.exec = nullptr;
+        }
+    }
+    if (!updated) {
+        ce = cudaGraphInstantiate(&b.exec, g, 0);
+        if (ce != cudaSuccess) {
+            cudaGraphDestroy(g);
+            return set_err("graph instantiate: %s", cudaGetErrorString(ce)), WW_ERR_CUDA;
+        }
+    }
+    cudaGraphDestroy(g);
+    WW_CU(cudaGraphLaunch(b.exec, st));
+    return WW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ww_batch_configs(ww_batch_cfg *out, uint32_t cap, uint32_t *n) {
+    if (!n || (!out && cap)) return WW_ERR_ARG;
+    const auto &t = configs();
+    *n = (uint32_t)t.size();
+    for (uint32_t i = 0; i < cap && i < t.size(); ++i)
+        out[i] = ww_batch_cfg{(uint32_t)t[i].seg_words, (uint32_t)t[i].threads, (uint32_t)t[i].ppt, 0};
+    return WW_OK;
+}
+
+int ww_batch_set_config(ww_ctx *ctx, const ww_batch_cfg *cfg) {
+    if (!ctx || !cfg) return set_err("null argument"), WW_ERR_ARG;
+    if (!find_cfg(*cfg)) return set_err("config %u/%u/%u is not compiled", cfg->seg_words, cfg->threads, cfg->ppt),
+                                WW_ERR_ARG;
+    BatchState *&bs = ctx_batch(ctx);
+    if (!bs) bs = new (std::nothrow) BatchState;
+    if (!bs) return set_err("host allocation failed"), WW_ERR_NOMEM;
+    bs->cfg = *cfg;
+    bs->tuned = true;
+    return WW_OK;
+}
+
+int ww_batch_get_config(ww_ctx *ctx, ww_batch_cfg *cfg) {
+    if (!ctx || !cfg) return set_err("null argument"), WW_ERR_ARG;
+    BatchState *bs = ctx_batch(ctx);
+    *cfg = bs ? bs->cfg : default_cfg();
+    return WW_OK;
+}
+
+int ww_batch_reserve_hits(ww_ctx *ctx, uint32_t max_hits) {
+    if (!ctx || max_hits == 0) return set_err("bad argument"), WW_ERR_ARG;
+    BatchState *&bs = ctx_batch(ctx);
+    if (!bs) bs = new (std::nothrow) BatchState;
+    if (!bs) return set_err("host allocation failed"), WW_ERR_NOMEM;
+    cudaSetDevice(ctx_device(ctx));
+    return ensure_capacity(*bs, 1, max_hits);
+}
+
+int ww_batch_submit(ww_ctx *ctx, const ww_unit *units, uint32_t n) {
+    if (!ctx || (!units && n)) return set_err("null argument"), WW_ERR_ARG;
+    BatchState *&bs = ctx_batch(ctx);
+    if (!bs) bs = new (std::nothrow) BatchState;
+    if (!bs) return set_err("host allocation failed"), WW_ERR_NOMEM;
+    WW_CU(cudaSetDevice(ctx_device(ctx)));
+    const CfgEntry *e = find_cfg(bs->cfg);
+    if (!e) return set_err("no batch config"), WW_ERR_STATE;
+    u64 tiles = 0;
+    return run_batch(ctx, *bs, units, n, *e, &tiles);
+}
+
+int ww_batch_collect(ww_ctx *ctx, ww_unit_result *out, uint32_t n, uint32_t *hit_count) {
+    if (!ctx || (!out && n)) return set_err("null argument"), WW_ERR_ARG;
+    BatchState *bs = ctx_batch(ctx);
+    if (!bs || n > bs->n_units) return set_err("no batch of %u units submitted", n), WW_ERR_STATE;
+    cudaStream_t st = (cudaStream_t)ctx_stream(ctx);
+    u32 hc[2] = {0, 0};
+    if (n) WW_CU(cudaMemcpyAsync(bs->h_units, bs->d_units, (size_t)n * sizeof(UnitState), cudaMemcpyDeviceToHost, st));
+    WW_CU(cudaMemcpyAsync(&hc[0], bs->d_hit_count, 4, cudaMemcpyDeviceToHost, st));
+    WW_CU(cudaMemcpyAsync(&hc[1], bs->d_overflow, 4, cudaMemcpyDeviceToHost, st));
+    WW_CU(cudaStreamSynchronize(st));
+    for (uint32_t i = 0; i < n; ++i) {
+        out[i].checksum = bs->h_units[i].checksum;
+        out[i].prp_count = bs->h_units[i].prp_count;
+        out[i].hits = bs->h_units[i].hits;
+        out[i].tiles_done = bs->h_units[i].tiles_done;
+    }
+    if (hit_count) *hit_count = hc[0];
+    if (hc[1] & 2) return set_err("%u hits, buffer holds %u", hc[0], bs->hit_cap), WW_ERR_HIT_OVERFLOW;
+    return WW_OK;
+}
+
+int ww_batch_run(ww_ctx *ctx, const ww_unit *units, uint32_t n, ww_unit_result *out) {
+    int rc = ww_batch_submit(ctx, units, n);
+    if (rc) return rc;
+    uint32_t hits = 0;
+    return ww_batch_collect(ctx, out, n, &hits);
+}
+
+int ww_batch_hits(ww_ctx *ctx, ww_hit *out, uint32_t *unit_of_hit, uint32_t cap, uint32_t *n) {
+    if (!ctx || !n || (!out && cap)) return set_err("null argument"), WW_ERR_ARG;
+    BatchState *bs = ctx_batch(ctx);
+    if (!bs || !bs->d_hit_count) return set_err("no batch submitted"), WW_ERR_STATE;
+    u32 cnt = 0;
+    WW_CU(cudaMemcpy(&cnt, bs->d_hit_count, 4, cudaMemcpyDeviceToHost));
+    *n = cnt;
+    u32 m = std::min(std::min(cnt, bs->hit_cap), cap);
+    if (m) {
+        std::vector<u64> p(m);
+        std::vector<int> r(m), rem(m), q(m);
+        std::vector<u32> u(m);
+        WW_CU(cudaMemcpy(p.data(), bs->d_hit_p, (size_t)m * 8, cudaMemcpyDeviceToHost));
+        WW_CU(cudaMemcpy(r.data(), bs->d_hit_res, (size_t)m * 4, cudaMemcpyDeviceToHost));
+        WW_CU(cudaMemcpy(rem.data(), bs->d_hit_rem, (size_t)m * 4, cudaMemcpyDeviceToHost));
+        WW_CU(cudaMemcpy(q.data(), bs->d_hit_quot, (size_t)m * 4, cudaMemcpyDeviceToHost));
+        WW_CU(cudaMemcpy(u.data(), bs->d_hit_unit, (size_t)m * 4, cudaMemcpyDeviceToHost));
+        for (u32 i = 0; i < m; ++i) {
+            out[i] = ww_hit{p[i], r[i], rem[i], q[i], 0};
+            if (unit_of_hit) unit_of_hit[i] = u[i];
+        }
+    }
+    if (cnt > bs->hit_cap) return set_err("%u hits, buffer holds %u", cnt, bs->hit_cap), WW_ERR_HIT_OVERFLOW;
+    return WW_OK;
+}
+
+// Time every compiled configuration on the sample (after one warm-up run
+// each) and keep the fastest in the context.
+int ww_batch_tune(ww_ctx *ctx, const ww_unit *sample, uint32_t n, ww_batch_cfg *best, float *best_ms) {
+    if (!ctx || !sample || n == 0) return set_err("bad argument"), WW_ERR_ARG;
+    BatchState *&bs = ctx_batch(ctx);
+    if (!bs) bs = new (std::nothrow) BatchState;
+    if (!bs) return set_err("host allocation failed"), WW_ERR_NOMEM;
+    WW_CU(cudaSetDevice(ctx_device(ctx)));
+    cudaStream_t st = (cudaStream_t)ctx_stream(ctx);
+    cudaEvent_t a, b;
+    WW_CU(cudaEventCreate(&a));
+    WW_CU(cudaEventCreate(&b));
+    float bestv = 1e30f;
+    ww_batch_cfg bestc = default_cfg();
+    for (const CfgEntry &e : configs()) {
+        u64 tiles = 0;
+        int rc = run_batch(ctx, *bs, sample, n, e, &tiles);  // warm-up (also instantiates)
+        if (rc == WW_ERR_ARG) continue;                      // does not fit
+        if (rc) return rc;
+        cudaEventRecord(a, st);
+        rc = run_batch(ctx, *bs, sample, n, e, &tiles);
+        if (rc) return rc;
+        cudaEventRecord(b, st);
+        WW_CU(cudaEventSynchronize(b));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms < bestv) {
+            bestv = ms;
+            bestc = ww_batch_cfg{(uint32_t)e.seg_words, (uint32_t)e.threads, (uint32_t)e.ppt, 0};
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    bs->cfg = bestc;
+    bs->tuned = true;
+    if (best) *best = bestc;
+    if (best_ms) *best_ms = bestv;
+    return WW_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Request server: continuous batching over device slots.
+
+namespace ww {
+struct ServerState;
+ServerState *&ctx_server(ww_ctx *c);
+}
+
+namespace ww {
+
+struct ServerReq {
+    ww_request r;
+    double t_submit;
+};
+
+struct ServerSlot {
+    bool busy = false;
+    ww_request r{};
+    double t_submit = 0, t_admit = 0;
+    u64 pool_off = 0, pool_len = 0;  // bytes
+};
+
+struct ServerState {
+    ww_server_cfg cfg{};
+    const CfgEntry *e = nullptr;
+    int grid = 0;
+    UnitState *d_slots = nullptr, *h_slots = nullptr;
+    u64 *pool = nullptr;
+    u32 *d_rr = nullptr, *d_epoch = nullptr, *d_hit_count = nullptr, *d_overflow = nullptr;
+    u32 *d_hit_unit = nullptr, *h_hit_unit = nullptr;
+    u64 *d_hit_p = nullptr, *h_hit_p = nullptr;
+    int *d_hit_res = nullptr, *d_hit_rem = nullptr, *d_hit_quot = nullptr;
+    int *h_hit_res = nullptr, *h_hit_rem = nullptr, *h_hit_quot = nullptr;
+    u32 *h_counts = nullptr;  // pinned: hit count, overflow
+    std::vector<ServerSlot> slots;
+    std::deque<ServerReq> queue;
+    std::map<u64, u64> free_blocks;  // offset -> length (bytes), coalesced
+    u64 pool_used = 0;
+    std::map<u64, std::vector<ww_hit>> hits;       // per request id, finished + running
+    std::map<u64, std::pair<u64, u64>> done_prps;  // id -> (pool offset, count) until next step
+
+    ~ServerState() {
+        cudaFree(d_slots);
+        cudaFree(pool);
+        cudaFree(d_rr);
+        cudaFree(d_epoch);
+        cudaFree(d_hit_count);
+        cudaFree(d_overflow);
+        cudaFree(d_hit_unit);
+        cudaFree(d_hit_p);
+        cudaFree(d_hit_res);
+        cudaFree(d_hit_rem);
+        cudaFree(d_hit_quot);
+        if (h_slots) cudaFreeHost(h_slots);
+        if (h_hit_unit) cudaFreeHost(h_hit_unit);
+        if (h_hit_p) cudaFreeHost(h_hit_p);
+        if (h_hit_res) cudaFreeHost(h_hit_res);
+        if (h_hit_rem) cudaFreeHost(h_hit_rem);
+        if (h_hit_quot) cudaFreeHost(h_hit_quot);
+        if (h_counts) cudaFreeHost(h_counts);
+    }
+
+    // first fit over the coalesced free list
+    bool alloc(u64 len, u64 &off) {
+        if (len == 0) {
+            off = 0;
+            return true;
+        }
+        for (auto it = free_blocks.begin(); it != free_blocks.end(); ++it) {
+            if (it->second >= len) {
+                off = it->first;
+                const u64 rest = it->second - len;
+                const u64 roff = it->first + len;
+                free_blocks.erase(it);
+                if (rest) free_blocks[roff] = rest;
+                pool_used += len;
+                return true;
+            }
+        }
+        return false;
+    }
+    void release(u64 off, u64 len) {
+        if (len == 0) return;
+        pool_used -= len;
+        auto it = free_blocks.emplace(off, len).first;
+        auto nx = std::next(it);
+        if (nx != free_blocks.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_blocks.erase(nx);
+        }
+        if (it != free_blocks.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_blocks.erase(it);
+            }
+        }
+    }
+};
+
+void destroy_server_state(ServerState *s) { delete s; }
+
+}  // namespace ww
+
+namespace {
+
+double mono_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+extern "C" {
+
+int ww_server_open(ww_ctx *ctx, const ww_server_cfg *cfg) {
+    if (!ctx || !cfg || cfg->max_active == 0 || cfg->epoch_tiles == 0 || cfg->max_hits == 0)
+        return set_err("bad server configuration"), WW_ERR_ARG;
+    WW_CU(cudaSetDevice(ctx_device(ctx)));
+    ServerState *&sv = ctx_server(ctx);
+    delete sv;
+    sv = new (std::nothrow) ServerState;
+    if (!sv) return set_err("host allocation failed"), WW_ERR_NOMEM;
+    ServerState &s = *sv;
+    s.cfg = *cfg;
+    ww_batch_cfg bc = default_cfg();
+    if (BatchState *bs = ctx_batch(ctx)) bc = bs->cfg;  // the tuned configuration, if any
+    s.e = find_cfg(bc);
+    if (!s.e) return set_err("no tile configuration"), WW_ERR_STATE;
+    WW_CU(cudaFuncSetAttribute(s.e->serve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.e->smem));
+    int per_sm = 0, sms = 0;
+    WW_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s.e->serve_kernel, s.e->threads, s.e->smem));
+    WW_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx_device(ctx)));
+    s.grid = std::max(1, per_sm) * sms;
+    const u32 n = cfg->max_active, h = cfg->max_hits;
+    WW_CU(cudaMalloc(&s.d_slots, (size_t)n * sizeof(UnitState)));
+    WW_CU(cudaMallocHost(&s.h_slots, (size_t)n * sizeof(UnitState)));
+    memset(s.h_slots, 0, (size_t)n * sizeof(UnitState));
+    WW_CU(cudaMemcpy(s.d_slots, s.h_slots, (size_t)n * sizeof(UnitState), cudaMemcpyHostToDevice));
+    if (cfg->prp_pool_bytes) {
+        WW_CU(cudaMalloc(&s.pool, cfg->prp_pool_bytes));
+        s.free_blocks[0] = cfg->prp_pool_bytes & ~7ull;
+    }
+    WW_CU(cudaMalloc(&s.d_rr, 4));
+    WW_CU(cudaMalloc(&s.d_epoch, 4));
+    WW_CU(cudaMalloc(&s.d_hit_count, 4));
+    WW_CU(cudaMalloc(&s.d_overflow, 4));
+    WW_CU(cudaMemset(s.d_rr, 0, 4));
+    WW_CU(cudaMalloc(&s.d_hit_unit, (size_t)h * 4));
+    WW_CU(cudaMalloc(&s.d_hit_p, (size_t)h * 8));
+    WW_CU(cudaMalloc(&s.d_hit_res, (size_t)h * 4));
+    WW_CU(cudaMalloc(&s.d_hit_rem, (size_t)h * 4));
+    WW_CU(cudaMalloc(&s.d_hit_quot, (size_t)h * 4));
+    WW_CU(cudaMallocHost(&s.h_hit_unit, (size_t)h * 4));
+    WW_CU(cudaMallocHost(&s.h_hit_p, (size_t)h * 8));
+    WW_CU(cudaMallocHost(&s.h_hit_res, (size_t)h * 4));
+    WW_CU(cudaMallocHost(&s.h_hit_rem, (size_t)h * 4));
+    WW_CU(cudaMallocHost(&s.h_hit_quot, (size_t)h * 4));
+    WW_CU(cudaMallocHost(&s.h_counts, 8));
+    s.slots.assign(n, ServerSlot());
+    return WW_OK;
+}
+
+int ww_server_close(ww_ctx *ctx) {
+    if (!ctx) return set_err("null ctx"), WW_ERR_ARG;
+    ServerState *&sv = ctx_server(ctx);
+    if (sv) cudaStreamSynchronize((cudaStream_t)ctx_stream(ctx));
+    delete sv;
+    sv = nullptr;
+    return WW_OK;
+}
+
+int ww_server_submit(ww_ctx *ctx, const ww_request *reqs, uint32_t n) {
+    ServerState *sv = ctx ? ctx_server(ctx) : nullptr;
+    if (!sv) return set_err("server not open"), WW_ERR_STATE;
+    if (!reqs && n) return set_err("null requests"), WW_ERR_ARG;
+    const double t = mono_s();
+    for (uint32_t i = 0; i < n; ++i) {
+        if (reqs[i].end <= reqs[i].start || reqs[i].start < 127)
+            return set_err("request %llu: bad range", (unsigned long long)reqs[i].id), WW_ERR_ARG;
+        sv->queue.push_back(ServerReq{reqs[i], t});
+    }
+    return WW_OK;
+}
+
+int ww_server_status(ww_ctx *ctx, uint32_t *queued, uint32_t *active, uint64_t *pool_used) {
+    ServerState *sv = ctx ? ctx_server(ctx) : nullptr;
+    if (!sv) return set_err("server not open"), WW_ERR_STATE;
+    uint32_t a = 0;
+    for (const ServerSlot &s : sv->slots) a += s.busy ? 1 : 0;
+    if (queued) *queued = (uint32_t)sv->queue.size();
+    if (active) *active = a;
+    if (pool_used) *pool_used = sv->pool_used;
+    return WW_OK;
+}
+
+int ww_server_step(ww_ctx *ctx, ww_request_result *done, uint32_t cap, uint32_t *ndone) {
+    ServerState *sv = ctx ? ctx_server(ctx) : nullptr;
+    if (!sv) return set_err("server not open"), WW_ERR_STATE;
+    if (!ndone || (!done && cap)) return set_err("null argument"), WW_ERR_ARG;
+    *ndone = 0;
+    ServerState &s = *sv;
+    cudaStream_t st = (cudaStream_t)ctx_stream(ctx);
+    const u64 tile = 64ull * (u64)s.e->seg_words;
+    s.done_prps.clear();
+
+    // ---- admission: FIFO while a slot and PRP-buffer memory are free
+    const u32 n = s.cfg.max_active;
+    bool changed = false;
+    for (u32 k = 0; k < n && !s.queue.empty(); ++k) {
+        if (s.slots[k].busy) continue;
+        const ServerReq &q = s.queue.front();
+        const u64 bound = ww_prp_count_bound(q.r.start, q.r.end);
+        const u64 len = s.cfg.store_prps ? bound * 8 : 0;
+        u64 off = 0;
+        if (len > s.cfg.prp_pool_bytes && s.cfg.store_prps)
+            return set_err("request %llu needs %llu bytes, pool has %llu", (unsigned long long)q.r.id,
+                           (unsigned long long)len, (unsigned long long)s.cfg.prp_pool_bytes), WW_ERR_NOMEM;
+        if (!s.alloc(len, off)) break;  // wait for memory
+        ServerSlot &sl = s.slots[k];
+        sl.busy = true;
+        sl.r = q.r;
+        sl.t_submit = q.t_submit;
+        sl.t_admit = mono_s();
+        sl.pool_off = off;
+        sl.pool_len = len;
+        UnitState &u = s.h_slots[k];
+        memset(&u, 0, sizeof u);
+        u.start = q.r.start;
+        u.end = q.r.end;
+        const u64 w = q.r.end - q.r.start;
+        u.n_tiles = w / tile + (w % tile ? 1 : 0);
+        u.active = 1;
+        if (s.cfg.store_prps) {
+            u.prp_out = s.pool + off / 8;
+            u.prp_cap = bound;
+        }
+        s.queue.pop_front();
+        changed = true;
+    }
+    u32 active = 0;
+    for (const ServerSlot &sl : s.slots) active += sl.busy ? 1 : 0;
+    if (active == 0) return WW_OK;
+
+    // ---- one epoch over every admitted request
+    if (changed)
+        WW_CU(cudaMemcpyAsync(s.d_slots, s.h_slots, (size_t)n * sizeof(UnitState), cudaMemcpyHostToDevice, st));
+    WW_CU(cudaMemsetAsync(s.d_epoch, 0, 4, st));
+    WW_CU(cudaMemsetAsync(s.d_hit_count, 0, 4, st));
+    WW_CU(cudaMemsetAsync(s.d_overflow, 0, 4, st));
+    BatchArgs a;
+    memset(&a, 0, sizeof a);
+    a.units = s.d_slots;
+    a.n_units = n;
+    a.rr = s.d_rr;
+    a.epoch_tiles = s.d_epoch;
+    a.budget = s.cfg.epoch_tiles;
+    a.hit_p = s.d_hit_p;
+    a.hit_result = s.d_hit_res;
+    a.hit_rem = s.d_hit_rem;
+    a.hit_quot = s.d_hit_quot;
+    a.hit_unit = s.d_hit_unit;
+    a.hit_count = s.d_hit_count;
+    a.hit_capacity = s.cfg.max_hits;
+    a.overflow = s.d_overflow;
+    const int grid = std::min<int>(s.grid, (int)s.cfg.epoch_tiles);
+    s.e->serve_kernel<<<grid, s.e->threads, s.e->smem, st>>>(a);
+    WW_CU(cudaGetLastError());
+    WW_CU(cudaMemcpyAsync(s.h_slots, s.d_slots, (size_t)n * sizeof(UnitState), cudaMemcpyDeviceToHost, st));
+    WW_CU(cudaMemcpyAsync(s.h_counts, s.d_hit_count, 4, cudaMemcpyDeviceToHost, st));
+    WW_CU(cudaMemcpyAsync(s.h_counts + 1, s.d_overflow, 4, cudaMemcpyDeviceToHost, st));
+    WW_CU(cudaStreamSynchronize(st));
+    const u32 nh = std::min(s.h_counts[0], s.cfg.max_hits);
+    if (nh) {
+        WW_CU(cudaMemcpy(s.h_hit_unit, s.d_hit_unit, (size_t)nh * 4, cudaMemcpyDeviceToHost));
+        WW_CU(cudaMemcpy(s.h_hit_p, s.d_hit_p, (size_t)nh * 8, cudaMemcpyDeviceToHost));
+        WW_CU(cudaMemcpy(s.h_hit_res, s.d_hit_res, (size_t)nh * 4, cudaMemcpyDeviceToHost));
+        WW_CU(cudaMemcpy(s.h_hit_rem, s.d_hit_rem, (size_t)nh * 4, cudaMemcpyDeviceToHost));
+        WW_CU(cudaMemcpy(s.h_hit_quot, s.d_hit_quot, (size_t)nh * 4, cudaMemcpyDeviceToHost));
+        for (u32 i = 0; i < nh; ++i) {
+            const u32 k = s.h_hit_unit[i];
+            if (k < n && s.slots[k].busy)
+                s.hits[s.slots[k].r.id].push_back(
+                    ww_hit{s.h_hit_p[i], s.h_hit_res[i], s.h_hit_rem[i], s.h_hit_quot[i], 0});
+        }
+    }
+    const bool hit_overflow = (s.h_counts[1] & 2) != 0;
+
+    // ---- finished requests
+    const double t = mono_s();
+    bool freed = false;
+    for (u32 k = 0; k < n; ++k) {
+        ServerSlot &sl = s.slots[k];
+        UnitState &u = s.h_slots[k];
+        if (!sl.busy || u.tiles_done < u.n_tiles) continue;
+        if (*ndone < cap) {
+            ww_request_result &r = done[*ndone];
+            r.id = sl.r.id;
+            r.checksum = u.checksum;
+            r.prp_count = u.prp_count;
+            r.prps_stored = u.prp_out ? std::min(u.prp_written, u.prp_cap) : 0;
+            r.hits = u.hits;
+            r.status = hit_overflow ? WW_ERR_HIT_OVERFLOW : (u.prp_written > u.prp_cap && u.prp_out ? WW_ERR_PRP_OVERFLOW : WW_OK);
+            r.t_submit = sl.t_submit;
+            r.t_admit = sl.t_admit;
+            r.t_done = t;
+            ++*ndone;
+        } else {
+            continue;  // reported at the next step
+        }
+        if (u.prp_out) s.done_prps[sl.r.id] = std::make_pair(sl.pool_off, std::min(u.prp_written, u.prp_cap));
+        s.release(sl.pool_off, sl.pool_len);
+        sl.busy = false;
+        memset(&u, 0, sizeof u);
+        freed = true;
+    }
+    if (freed)
+        WW_CU(cudaMemcpyAsync(s.d_slots, s.h_slots, (size_t)n * sizeof(UnitState), cudaMemcpyHostToDevice, st));
+    return WW_OK;
+}
+
+int ww_server_hits(ww_ctx *ctx, uint64_t id, ww_hit *out, uint32_t cap, uint32_t *n) {
+    ServerState *sv = ctx ? ctx_server(ctx) : nullptr;
+    if (!sv) return set_err("server not open"), WW_ERR_STATE;
+    if (!n || (!out && cap)) return set_err("null argument"), WW_ERR_ARG;
+    auto it = sv->hits.find(id);
+    *n = 0;
+    if (it == sv->hits.end()) return WW_OK;
+    *n = (uint32_t)it->second.size();
+    for (uint32_t i = 0; i < cap && i < it->second.size(); ++i) out[i] = it->second[i];
+    sv->hits.erase(it);
+    return WW_OK;
+}
+
+int ww_server_prps(ww_ctx *ctx, uint64_t id, uint64_t *out, uint64_t cap, uint64_t *n) {
+    ServerState *sv = ctx ? ctx_server(ctx) : nullptr;
+    if (!sv) return set_err("server not open"), WW_ERR_STATE;
+    if (!n || (!out && cap)) return set_err("null argument"), WW_ERR_ARG;
+    auto it = sv->done_prps.find(id);
+    if (it == sv->done_prps.end()) return set_err("no stored PRP list for request %llu", (unsigned long long)id),
+                                          WW_ERR_STATE;
+    *n = it->second.second;
+    const u64 m = std::min<u64>(cap, it->second.second);
+    if (m) WW_CU(cudaMemcpy(out, sv->pool + it->second.first / 8, m * 8, cudaMemcpyDeviceToHost));
+    return WW_OK;
+}
+
+}  // extern "C"

@@ -191,6 +191,7 @@ int ww_launch_digits(const uint64_t *primes, uint64_t n, uint64_t *out, void *st
 
 }  // extern "C"
 
+
 // ------------------------------------------------------------------ context
 
 namespace {
@@ -207,7 +208,16 @@ __global__ void k_set_count(unsigned int *pc, unsigned int v) { pc[0] = v; }
 
 }  // namespace
 
+namespace ww {
+struct BatchState;
+struct ServerState;
+void destroy_batch_state(BatchState *s);
+void destroy_server_state(ServerState *s);
+}  // namespace ww
+
 struct ww_ctx {
+    ww::BatchState *batch = nullptr;
+    ww::ServerState *server = nullptr;
     int device = 0;
     cudaStream_t stream = nullptr;
     DevCounters *dc = nullptr;
@@ -250,6 +260,8 @@ void ww_close(ww_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    ww::destroy_server_state(c->server);
+    ww::destroy_batch_state(c->batch);
     cudaFree(c->prime);
     cudaFree(c->inv);
     cudaFree(c->one);
@@ -502,3 +514,10 @@ int ww_read_prps(ww_ctx *c, uint64_t *out, uint64_t cap, uint64_t *n) {
 }
 
 }  // extern "C"
+
+namespace ww {
+int ctx_device(ww_ctx *c) { return c->device; }
+void *ctx_stream(ww_ctx *c) { return c->stream; }
+BatchState *&ctx_batch(ww_ctx *c) { return c->batch; }
+ServerState *&ctx_server(ww_ctx *c) { return c->server; }
+}  // namespace ww

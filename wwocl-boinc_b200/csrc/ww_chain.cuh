@@ -274,3 +274,71 @@ WW_HD D2 m2_redc32(D2 x, const P32 &P) {
 }
 
 }  // namespace ww
+
+namespace ww {
+
+// ---------------------------------------------------------------------------
+// The same two-digit arithmetic written for IMAD.WIDE.U32: every 32x32
+// partial product is formed as (u64)a * b + c with a 64-bit addend, which
+// cannot overflow when c is the sum of at most two 32-bit words
+// ((2^32-1)^2 + 2(2^32-1) = 2^64-1), so the carries ride inside the wide
+// products instead of separate add-with-carry instructions.
+
+WW_HD void mul64w(u64 a, u64 b, u64 &lo, u64 &hi) {
+    const u32 a0 = lo32(a), a1 = hi32(a), b0 = lo32(b), b1 = hi32(b);
+    const u64 t0 = (u64)a0 * b0;
+    const u64 t1 = (u64)a0 * b1 + (t0 >> 32);
+    const u64 t2 = (u64)a1 * b0 + (u32)t1;
+    hi = (u64)a1 * b1 + (t1 >> 32) + (t2 >> 32);
+    lo = (t2 << 32) | (u32)t0;
+}
+
+WW_HD u64 mulhi64w(u64 a, u64 b) {
+    u64 lo, hi;
+    mul64w(a, b, lo, hi);
+    return hi;
+}
+
+// Finish of a product with 64-bit q = p^-1 reductions (the formulation of
+// m2_finish, wide products).
+WW_HD D2 m2_finish_w(u64 alo, u64 ahi, u64 clo, u64 chi, u64 ctop, u64 p, u64 q) {
+    const u64 u = alo * q;
+    const u64 v = mulhi64w(u, p);
+    D2 r;
+    const bool b = ahi < v;
+    r.d0 = ahi - v + (b ? p : 0);
+    u64 s = clo + u;
+    const u64 c = s < clo;
+    u64 h = chi + c;
+    ctop += (h < c);
+    if (ctop | (h >= p)) h -= p;
+    const u64 v2 = mulhi64w(s * q, p);
+    const u64 t = v2 + (u64)b;
+    r.d1 = h - t + (h < t ? p : 0);
+    return r;
+}
+
+WW_HD D2 m2_mul_w(D2 x, D2 y, u64 p, u64 q) {
+    u64 alo, ahi, l1, h1, l2, h2;
+    mul64w(x.d0, y.d0, alo, ahi);
+    mul64w(x.d0, y.d1, l1, h1);
+    mul64w(x.d1, y.d0, l2, h2);
+    const u64 clo = l1 + l2;
+    const u64 c = clo < l1;
+    u64 chi = h1 + h2;
+    u64 ctop = chi < h1;
+    chi += c;
+    ctop += chi < c;
+    return m2_finish_w(alo, ahi, clo, chi, ctop, p, q);
+}
+
+WW_HD D2 m2_sqr_w(D2 x, u64 p, u64 q) {
+    u64 alo, ahi, l, h;
+    mul64w(x.d0, x.d0, alo, ahi);
+    mul64w(x.d0, x.d1, l, h);
+    return m2_finish_w(alo, ahi, l << 1, (h << 1) | (l >> 63), h >> 63, p, q);
+}
+
+WW_HD D2 m2_redc_w(D2 x, u64 p, u64 q) { return m2_finish_w(x.d0, 0, x.d1, 0, 0, p, q); }
+
+}  // namespace ww

@@ -1,0 +1,147 @@
+// ww_device.cuh -- device helpers shared by the kernels of the WWocl search
+// path on sm_100a (the kernels themselves are in ww_kernels.cuh and
+// ww_batch.cuh).
+
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "ww_deep.cuh"
+#include "ww_tests.cuh"
+
+namespace ww {
+
+constexpr int kSegWords = 4096;               // bitmap words per segment (16 KB)
+constexpr int kSegOdd = kSegWords * 32;       // odd numbers per segment
+constexpr int kSieveThreads = 256;
+constexpr int kSieveWarps = kSieveThreads / 32;
+constexpr int kWordsPerThread = kSegWords / kSieveThreads;
+constexpr int kWordsPerWarp = kSegWords / kSieveWarps;
+constexpr int kQueueCap = 640;  // 31 carried + 32 words x at most 18 survivors
+constexpr int kTestThreads = 256;
+#ifndef WW_TEST_MINB
+#define WW_TEST_MINB 1  // minimum resident CTAs per SM asked of the test kernels
+#endif
+
+struct HitOut {
+    u64 *prime;
+    int *rem, *quot, *result;
+    u32 *count;
+    u32 capacity;
+    u32 *overflow;
+};
+
+__device__ __forceinline__ void emit_hit(const HitOut &h, u64 p, int result, int rem, int quot) {
+    const u32 ix = atomicAdd(h.count, 1u);
+    if (ix < h.capacity) {
+        h.prime[ix] = p;
+        h.result[ix] = result;
+        h.rem[ix] = rem;
+        h.quot[ix] = quot;
+    } else {
+        atomicOr(h.overflow, 2u);
+    }
+}
+
+__device__ __forceinline__ u64 warp_sum(u64 v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ------------------------------------------------------------------ sieve
+
+// Composite mask of one prime r for a word whose first bit is at j0 (bit j
+// of the word is the odd number n_w + 2j; r divides n_w + 2 j0).
+template <u32 R>
+__device__ __forceinline__ u32 prime_mask(u32 j0) {
+    if (R < 32) {
+        u32 pat = 0;
+#pragma unroll
+        for (u32 k = 0; k < 32; k += R) pat |= 1u << k;
+        return pat << j0;
+    }
+    return j0 < 32 ? (1u << (j0 & 31)) : 0u;
+}
+
+template <u32 R>
+__device__ __forceinline__ u32 first_hit(u64 n) {
+    // smallest j >= 0 with R | n + 2j
+    const u32 res = (u32)(n % R);
+    const u32 inv2 = (R + 1) / 2;
+    return ((R - res) % R) * inv2 % R;
+}
+
+template <u32 R>
+__device__ __forceinline__ void step_hit(u32 &j0) {
+    // next word: the index moves down by 32 (mod R)
+    const u32 d = 32 % R;
+    j0 = (j0 >= d) ? j0 - d : j0 + R - d;
+}
+
+#define WW_FOR_SMALL_PRIMES(X) \
+    X(3) X(5) X(7) X(11) X(13) X(17) X(19) X(23) X(29) X(31) X(37) X(41) X(43) X(47) X(53) \
+    X(59) X(61) X(67) X(71) X(73) X(79) X(83) X(89) X(97) X(101) X(103) X(107) X(109) X(113)
+
+// ------------------------------------------------------------- deep sieve
+// (the scheme is described in ww_deep.cuh)
+
+#define WW_DEEP_ROW4(r, m, a, b) {r, m, a, b},
+static __device__ const uint4 kDeepDev[WW_DEEP_COUNT] = {WW_DEEP_ROWS(WW_DEEP_ROW4)};
+
+// Rescue list of one segment, built from the small-prime bitmap before the
+// deep marking: bit indices j (odd number first + 2j) of multiples n = r
+// (mod r * ord_r(2)) that have no factor <= 113.  The count may exceed
+// kRescueCap; the caller then skips the deep marking for that segment.
+__device__ __forceinline__ void deep_collect(u64 first, u32 nvalid, const u32 *bitmap, u32 *rescue,
+                                             u32 *rescue_n, int tid, int nthreads) {
+    for (int i = tid; i < WW_DEEP_COUNT; i += nthreads) {
+        const uint4 e = kDeepDev[i];
+        const u64 step = deep_rescue_step(e.y);
+        for (u64 off = deep_first_rescue(first, e.x, e.y, e.w); (off >> 1) < nvalid; off += step) {
+            const u32 j = (u32)(off >> 1);
+            if (!((bitmap[j >> 5] >> (j & 31)) & 1u)) {
+                const u32 k = atomicAdd(rescue_n, 1u);
+                if (k < kRescueCap) rescue[k] = j;
+            }
+        }
+    }
+}
+
+// Mark every odd multiple of the deep primes in the segment.
+__device__ __forceinline__ void deep_mark(u64 first, u32 nvalid, u32 *bitmap, int tid, int nthreads) {
+    for (int i = tid; i < WW_DEEP_COUNT; i += nthreads) {
+        const uint4 e = kDeepDev[i];
+        for (u32 j = deep_first_multiple(first, e.x, e.z); j < nvalid; j += e.x)
+            atomicOr(&bitmap[j >> 5], 1u << (j & 31));
+    }
+}
+
+struct PrpOut {
+    u64 *prime, *inv;
+    u32 *count;
+    u64 capacity;
+    u32 *overflow;
+};
+
+__device__ __forceinline__ void sprp_emit(const PrpOut &out, u64 n, bool active) {
+    u64 q = 0;
+    const bool pass = active && prp_test(n, q);
+    const u32 ballot = __ballot_sync(0xffffffffu, pass);
+    if (ballot == 0) return;
+    const int lane = threadIdx.x & 31;
+    u32 base = 0;
+    if (lane == 0) base = atomicAdd(out.count, (u32)__popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (pass) {
+        const u64 ix = (u64)base + (u64)__popc(ballot & ((1u << lane) - 1u));
+        if (ix < out.capacity) {
+            out.prime[ix] = n;
+            out.inv[ix] = q;
+        } else {
+            atomicOr(out.overflow, 1u);
+        }
+    }
+}
+
+}  // namespace ww

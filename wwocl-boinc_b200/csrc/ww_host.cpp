@@ -231,9 +231,10 @@ int ww_selftest_range(uint64_t lo, uint64_t hi, uint64_t *prp_count, uint64_t *c
 // instantiation of the same source): op 0 product, 1 square, 2 leave
 // Montgomery form.  xy holds (x0, x1, y0, y1) per case, out (z0, z1).
 
-extern "C" int ww_selftest_m2(int op, uint64_t p, const uint64_t *xy, uint64_t n, uint64_t *out) {
-    if ((p & 1) == 0 || p < 3 || ((!xy || !out) && n) || op < 0 || op > 2) return WW_ERR_ARG;
-    const Arith32 ar(p, inv64(p));
+namespace {
+template <class A>
+void m2_cases(int op, uint64_t p, const uint64_t *xy, uint64_t n, uint64_t *out) {
+    const A ar(p, inv64(p));
     for (uint64_t i = 0; i < n; ++i) {
         const D2 x = {xy[4 * i], xy[4 * i + 1]};
         const D2 y = {xy[4 * i + 2], xy[4 * i + 3]};
@@ -241,5 +242,65 @@ extern "C" int ww_selftest_m2(int op, uint64_t p, const uint64_t *xy, uint64_t n
         out[2 * i] = z.d0;
         out[2 * i + 1] = z.d1;
     }
+}
+}  // namespace
+
+// impl (op >> 4): 0 = the kernels' policy, 1 = 64-bit C, 2 = PTX chains, 3 = wide.
+extern "C" int ww_selftest_m2(int op, uint64_t p, const uint64_t *xy, uint64_t n, uint64_t *out) {
+    const int impl = op >> 4;
+    op &= 15;
+    if ((p & 1) == 0 || p < 3 || ((!xy || !out) && n) || op < 0 || op > 2 || impl > 3) return WW_ERR_ARG;
+    switch (impl) {
+        case 1: m2_cases<Arith64>(op, p, xy, n, out); break;
+        case 2: m2_cases<Arith32>(op, p, xy, n, out); break;
+        case 3: m2_cases<ArithWide>(op, p, xy, n, out); break;
+        default: m2_cases<WW_ARITH>(op, p, xy, n, out); break;
+    }
+    return WW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Host emulation of the kernels' candidate generation (small primes 3..113,
+// then the deep sieve with its pseudoprime rescue list), one segment over
+// [lo, hi), for checking that the candidate set keeps every PRP.
+
+#include "ww_deep.cuh"
+
+namespace {
+#define WW_DEEP_ROWH(r, m, a, b) {r, m, a, b},
+const u32 kDeepHost[WW_DEEP_COUNT][4] = {WW_DEEP_ROWS(WW_DEEP_ROWH)};
+#undef WW_DEEP_ROWH
+}  // namespace
+
+extern "C" int ww_selftest_candidates(uint64_t lo, uint64_t hi, uint64_t *out, uint64_t cap, uint64_t *n,
+                                      uint64_t *rescued) {
+    if (!n || (!out && cap) || hi <= lo || lo < 127 || hi - lo > (1ull << 32)) return WW_ERR_ARG;
+    const u64 b0 = lo & ~1ull, first = b0 + 1;
+    const u64 nvalid = (hi - b0) / 2;
+    std::vector<u32> bitmap((nvalid + 31) / 32, 0);
+    auto mark = [&](u64 j) { bitmap[j >> 5] |= 1u << (j & 31); };
+    auto marked = [&](u64 j) { return (bitmap[j >> 5] >> (j & 31)) & 1u; };
+    static const u32 small[29] = {3,  5,  7,  11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53,
+                                  59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113};
+    for (u32 r : small)
+        for (u64 j = deep_first_multiple(first, r, (u32)((1ull << 32) % r)); j < nvalid; j += r) mark(j);
+    std::vector<u64> rescue;
+    for (int i = 0; i < WW_DEEP_COUNT; ++i) {
+        const u32 *e = kDeepHost[i];
+        for (u64 off = deep_first_rescue(first, e[0], e[1], e[3]); (off >> 1) < nvalid; off += deep_rescue_step(e[1]))
+            if (!marked(off >> 1)) rescue.push_back(off >> 1);
+    }
+    for (int i = 0; i < WW_DEEP_COUNT; ++i) {
+        const u32 *e = kDeepHost[i];
+        for (u64 j = deep_first_multiple(first, e[0], e[2]); j < nvalid; j += e[0]) mark(j);
+    }
+    std::vector<u64> cand;
+    for (u64 j = 0; j < nvalid; ++j)
+        if (!marked(j)) cand.push_back(first + 2 * j);
+    for (u64 j : rescue) cand.push_back(first + 2 * j);
+    std::sort(cand.begin(), cand.end());
+    *n = cand.size();
+    if (rescued) *rescued = rescue.size();
+    for (u64 i = 0; i < cap && i < cand.size(); ++i) out[i] = cand[i];
     return WW_OK;
 }

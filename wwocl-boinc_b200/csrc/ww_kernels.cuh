@@ -1,4 +1,4 @@
-// ww_kernels.cuh -- device code of the WWocl search path on sm_100a.
+// ww_kernels.cuh -- kernels of the WWocl search path on sm_100a.
 //
 //   k_sieve_prp   getsegprimes (getsegprimes.cl:228-301): one CTA per segment
 //                 of 2*kSegOdd integers.  The odd numbers of the segment form a
@@ -14,113 +14,17 @@
 //   k_digits      per-prime canonical digits (verification only).
 #pragma once
 
-#include <cuda_runtime.h>
-
-#include "ww_tests.cuh"
+#include "ww_device.cuh"
 
 namespace ww {
-
-constexpr int kSegWords = 4096;               // bitmap words per segment (16 KB)
-constexpr int kSegOdd = kSegWords * 32;       // odd numbers per segment
-constexpr int kSieveThreads = 256;
-constexpr int kSieveWarps = kSieveThreads / 32;
-constexpr int kWordsPerThread = kSegWords / kSieveThreads;
-constexpr int kWordsPerWarp = kSegWords / kSieveWarps;
-constexpr int kQueueCap = 640;  // 31 carried + 32 words x at most 18 survivors
-constexpr int kTestThreads = 256;
-
-struct HitOut {
-    u64 *prime;
-    int *rem, *quot, *result;
-    u32 *count;
-    u32 capacity;
-    u32 *overflow;
-};
-
-__device__ __forceinline__ void emit_hit(const HitOut &h, u64 p, int result, int rem, int quot) {
-    const u32 ix = atomicAdd(h.count, 1u);
-    if (ix < h.capacity) {
-        h.prime[ix] = p;
-        h.result[ix] = result;
-        h.rem[ix] = rem;
-        h.quot[ix] = quot;
-    } else {
-        atomicOr(h.overflow, 2u);
-    }
-}
-
-__device__ __forceinline__ u64 warp_sum(u64 v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// ------------------------------------------------------------------ sieve
-
-// Composite mask of one prime r for a word whose first bit is at j0 (bit j
-// of the word is the odd number n_w + 2j; r divides n_w + 2 j0).
-template <u32 R>
-__device__ __forceinline__ u32 prime_mask(u32 j0) {
-    if (R < 32) {
-        u32 pat = 0;
-#pragma unroll
-        for (u32 k = 0; k < 32; k += R) pat |= 1u << k;
-        return pat << j0;
-    }
-    return j0 < 32 ? (1u << (j0 & 31)) : 0u;
-}
-
-template <u32 R>
-__device__ __forceinline__ u32 first_hit(u64 n) {
-    // smallest j >= 0 with R | n + 2j
-    const u32 res = (u32)(n % R);
-    const u32 inv2 = (R + 1) / 2;
-    return ((R - res) % R) * inv2 % R;
-}
-
-template <u32 R>
-__device__ __forceinline__ void step_hit(u32 &j0) {
-    // next word: the index moves down by 32 (mod R)
-    const u32 d = 32 % R;
-    j0 = (j0 >= d) ? j0 - d : j0 + R - d;
-}
-
-#define WW_FOR_SMALL_PRIMES(X) \
-    X(3) X(5) X(7) X(11) X(13) X(17) X(19) X(23) X(29) X(31) X(37) X(41) X(43) X(47) X(53) \
-    X(59) X(61) X(67) X(71) X(73) X(79) X(83) X(89) X(97) X(101) X(103) X(107) X(109) X(113)
-
-struct PrpOut {
-    u64 *prime, *inv;
-    u32 *count;
-    u64 capacity;
-    u32 *overflow;
-};
-
-__device__ __forceinline__ void sprp_emit(const PrpOut &out, u64 n, bool active) {
-    u64 q = 0;
-    const bool pass = active && prp_test(n, q);
-    const u32 ballot = __ballot_sync(0xffffffffu, pass);
-    if (ballot == 0) return;
-    const int lane = threadIdx.x & 31;
-    u32 base = 0;
-    if (lane == 0) base = atomicAdd(out.count, (u32)__popc(ballot));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (pass) {
-        const u64 ix = (u64)base + (u64)__popc(ballot & ((1u << lane) - 1u));
-        if (ix < out.capacity) {
-            out.prime[ix] = n;
-            out.inv[ix] = q;
-        } else {
-            atomicOr(out.overflow, 1u);
-        }
-    }
-}
 
 // Sieve + SPRP over [lo, hi).  b0 = lo & ~1; segment s holds the odd numbers
 // b0 + 2(s*kSegOdd + j) + 1, j < kSegOdd.
 __global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out) {
     __shared__ u32 bitmap[kSegWords];
     __shared__ u32 queue[kSieveWarps][kQueueCap];
+    __shared__ u32 rescue[kRescueCap];
+    __shared__ u32 rescue_n;
     const u64 b0 = lo & ~1ull;
     const u64 span = hi - b0;
     const int lane = threadIdx.x & 31;
@@ -153,12 +57,25 @@ __global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64
                 bitmap[w] = m;
             }
         }
+        if (threadIdx.x == 0) rescue_n = 0;
         __syncthreads();
+
+        // ---- deep sieve 127..2^16 with the pseudoprime rescue list
+        const u64 nbase = b0 + seg_off + 1;
+        deep_collect(nbase, (u32)nvalid, bitmap, rescue, &rescue_n, threadIdx.x, kSieveThreads);
+        __syncthreads();
+        const u32 nresc = rescue_n <= (u32)kRescueCap ? rescue_n : 0u;
+        if (rescue_n <= (u32)kRescueCap) deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, kSieveThreads);
+        __syncthreads();
+        for (u32 base = warp * 32; base < nresc; base += kSieveWarps * 32) {
+            const bool act = base + lane < nresc;
+            const u32 j = act ? rescue[base + lane] : 0u;
+            sprp_emit(out, nbase + 2ull * j, act);
+        }
 
         // ---- per-warp compaction + SPRP, 32 candidates at a time
         u32 *q = queue[warp];
         int qn = 0;
-        const u64 nbase = b0 + seg_off + 1;
         for (int wb = warp * kWordsPerWarp; wb < (warp + 1) * kWordsPerWarp; wb += 32) {
             const int w = wb + lane;
             u32 cand = ~bitmap[w];
@@ -204,7 +121,7 @@ __device__ __forceinline__ void count_update(u32 *primecount, u64 *totalprimecou
     if (pc > primecount[1]) primecount[1] = pc;
 }
 
-__global__ void __launch_bounds__(kTestThreads) k_wieferich(u32 *primecount, const u64 *prime,
+__global__ void __launch_bounds__(kTestThreads, WW_TEST_MINB) k_wieferich(u32 *primecount, const u64 *prime,
                                                              const u64 *inv, u64 *g_one, HitOut hits,
                                                              u64 *checksum, u64 *totalprimecount,
                                                              u64 capacity) {
@@ -228,7 +145,7 @@ __global__ void __launch_bounds__(kTestThreads) k_wieferich(u32 *primecount, con
     if (blockIdx.x == 0 && threadIdx.x == 0) count_update(primecount, totalprimecount);
 }
 
-__global__ void __launch_bounds__(kTestThreads) k_wallsunsun(const u32 *primecount, const u64 *prime,
+__global__ void __launch_bounds__(kTestThreads, WW_TEST_MINB) k_wallsunsun(const u32 *primecount, const u64 *prime,
                                                               const u64 *inv, const u64 *g_one,
                                                               HitOut hits, u64 *checksum, u64 capacity) {
     const u64 n = min((u64)primecount[0], capacity);
@@ -252,7 +169,7 @@ __global__ void __launch_bounds__(kTestThreads) k_wallsunsun(const u32 *primecou
     if ((threadIdx.x & 31) == 0 && sum) atomicAdd(checksum, sum);
 }
 
-__global__ void __launch_bounds__(kTestThreads) k_test_prps(u32 *primecount, const u64 *prime,
+__global__ void __launch_bounds__(kTestThreads, WW_TEST_MINB) k_test_prps(u32 *primecount, const u64 *prime,
                                                              const u64 *inv, HitOut hits, u64 *checksum,
                                                              u64 *totalprimecount, u64 capacity) {
     const u64 n = min((u64)primecount[0], capacity);

@@ -2,9 +2,9 @@
 // reference's hit classification.
 //
 // The mod p^2 arithmetic is a policy: Arith64 uses 64-bit C products
-// (ww_arith.cuh), Arith32 the explicit 32-bit carry chains (ww_chain.cuh).
-// Both produce the same canonical digits; kernels and the host self-test
-// use WW_ARITH (Arith32 unless WW_ARITH_VERSION is 1).
+// (ww_arith.cuh), Arith32 explicit 32-bit PTX carry chains and ArithWide
+// 32x32+64 wide products (ww_chain.cuh).  All produce the same canonical
+// digits; kernels and the host self-test use WW_ARITH.
 #pragma once
 
 #include "ww_arith.cuh"
@@ -28,12 +28,25 @@ struct Arith32 {
     WW_HD D2 redc(D2 x) const { return m2_redc32(x, P); }
 };
 
-#if defined(WW_ARITH_VERSION) && WW_ARITH_VERSION == 1
-typedef Arith64 WW_ARITH;
-WW_HD bool prp_test(u64 n, u64 &q) { return sprp2(n, q); }
-#else
+struct ArithWide {
+    u64 p, q;
+    WW_HD ArithWide(u64 p_, u64 q_) : p(p_), q(q_) {}
+    WW_HD D2 mul(D2 x, D2 y) const { return m2_mul_w(x, y, p, q); }
+    WW_HD D2 sqr(D2 x) const { return m2_sqr_w(x, p, q); }
+    WW_HD D2 redc(D2 x) const { return m2_redc_w(x, p, q); }
+};
+
+// WW_ARITH_VERSION: 1 = 64-bit C products (default), 2 = PTX carry chains,
+// 3 = wide 32x32+64 products.  All three give identical digits.
+#if defined(WW_ARITH_VERSION) && WW_ARITH_VERSION == 2
 typedef Arith32 WW_ARITH;
 WW_HD bool prp_test(u64 n, u64 &q) { return sprp2_32(n, q); }
+#elif defined(WW_ARITH_VERSION) && WW_ARITH_VERSION == 3
+typedef ArithWide WW_ARITH;
+WW_HD bool prp_test(u64 n, u64 &q) { return sprp2(n, q); }
+#else
+typedef Arith64 WW_ARITH;
+WW_HD bool prp_test(u64 n, u64 &q) { return sprp2(n, q); }
 #endif
 
 WW_HD int top_bit(u64 x) {

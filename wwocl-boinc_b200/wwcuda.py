@@ -52,6 +52,38 @@ class Buffers(C.Structure):
                 ("prp_capacity", C.c_uint64), ("hit_capacity", C.c_uint32), ("stream", C.c_void_p)]
 
 
+class Unit(C.Structure):
+    _fields_ = [("start", C.c_uint64), ("end", C.c_uint64)]
+
+
+class UnitResult(C.Structure):
+    _fields_ = [("checksum", C.c_uint64), ("prp_count", C.c_uint64), ("hits", C.c_uint32),
+                ("tiles_done", C.c_uint32)]
+
+
+class BatchCfg(C.Structure):
+    _fields_ = [("seg_words", C.c_uint32), ("threads", C.c_uint32), ("ppt", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+    def as_tuple(self):
+        return (self.seg_words, self.threads, self.ppt)
+
+
+class Request(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("start", C.c_uint64), ("end", C.c_uint64)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("checksum", C.c_uint64), ("prp_count", C.c_uint64),
+                ("prps_stored", C.c_uint64), ("hits", C.c_uint32), ("status", C.c_int32),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]
+
+
+class ServerCfg(C.Structure):
+    _fields_ = [("prp_pool_bytes", C.c_uint64), ("max_active", C.c_uint32), ("epoch_tiles", C.c_uint32),
+                ("max_hits", C.c_uint32), ("store_prps", C.c_uint32)]
+
+
 _U64P = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 _VP = C.c_void_p
 _SIGS = {
@@ -94,7 +126,27 @@ _SIGS = {
     "ww_selftest_digits": (C.c_int, [_U64P, C.c_uint64, _U64P]),
     "ww_selftest_range": (C.c_int, [C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64),
                                     C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
+    "ww_batch_configs": (C.c_int, [C.POINTER(BatchCfg), C.c_uint32, C.POINTER(C.c_uint32)]),
+    "ww_batch_set_config": (C.c_int, [_VP, C.POINTER(BatchCfg)]),
+    "ww_batch_get_config": (C.c_int, [_VP, C.POINTER(BatchCfg)]),
+    "ww_batch_reserve_hits": (C.c_int, [_VP, C.c_uint32]),
+    "ww_batch_submit": (C.c_int, [_VP, C.POINTER(Unit), C.c_uint32]),
+    "ww_batch_collect": (C.c_int, [_VP, C.POINTER(UnitResult), C.c_uint32, C.POINTER(C.c_uint32)]),
+    "ww_batch_run": (C.c_int, [_VP, C.POINTER(Unit), C.c_uint32, C.POINTER(UnitResult)]),
+    "ww_batch_hits": (C.c_int, [_VP, C.POINTER(Hit), C.POINTER(C.c_uint32), C.c_uint32,
+                                C.POINTER(C.c_uint32)]),
+    "ww_batch_tune": (C.c_int, [_VP, C.POINTER(Unit), C.c_uint32, C.POINTER(BatchCfg),
+                                C.POINTER(C.c_float)]),
+    "ww_server_open": (C.c_int, [_VP, C.POINTER(ServerCfg)]),
+    "ww_server_close": (C.c_int, [_VP]),
+    "ww_server_submit": (C.c_int, [_VP, C.POINTER(Request), C.c_uint32]),
+    "ww_server_step": (C.c_int, [_VP, C.POINTER(RequestResult), C.c_uint32, C.POINTER(C.c_uint32)]),
+    "ww_server_status": (C.c_int, [_VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
+    "ww_server_hits": (C.c_int, [_VP, C.c_uint64, C.POINTER(Hit), C.c_uint32, C.POINTER(C.c_uint32)]),
+    "ww_server_prps": (C.c_int, [_VP, C.c_uint64, _VP, C.c_uint64, C.POINTER(C.c_uint64)]),
     "ww_selftest_m2": (C.c_int, [C.c_int, C.c_uint64, _U64P, C.c_uint64, _U64P]),
+    "ww_selftest_candidates": (C.c_int, [C.c_uint64, C.c_uint64, _U64P, C.c_uint64, C.POINTER(C.c_uint64),
+                                         C.POINTER(C.c_uint64)]),
     "ww_random_primes": (C.c_int, [C.c_int, C.c_uint64, C.c_uint64, _U64P, C.POINTER(C.c_uint64)]),
     "ww_pipe_bench": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
@@ -170,6 +222,14 @@ def selftest_m2(op: int, p: int, xy: np.ndarray) -> np.ndarray:
     out = np.zeros(2 * n, dtype=np.uint64)
     check(_L.ww_selftest_m2(op, p, xy, n, out), "ww_selftest_m2")
     return out.reshape(-1, 2)
+
+
+def selftest_candidates(lo: int, hi: int) -> tuple[np.ndarray, int]:
+    cap = (hi - lo) // 2 + 2
+    out = np.zeros(cap, dtype=np.uint64)
+    n, r = C.c_uint64(0), C.c_uint64(0)
+    check(_L.ww_selftest_candidates(lo, hi, out, cap, C.byref(n), C.byref(r)), "ww_selftest_candidates")
+    return out[: n.value], int(r.value)
 
 
 def random_primes(seed: int, n: int, device: int = 0) -> tuple[np.ndarray, int]:
@@ -291,6 +351,8 @@ class Context:
         """Plain path over [lo, hi): clear, then per segment clearn -> sieve -> tests."""
         self.clear_results()
         seg = segment or hi - lo
+        while seg > 1 and prp_count_bound(0, seg) > self.max_prps:  # keep every launch inside the buffer
+            seg //= 2
         start = lo
         while start < hi:
             stop = min(start + seg, hi)
@@ -306,6 +368,142 @@ class Context:
         c = self.counters()
         c["hits"] = [] if c["overflow"] & 2 else self.hits()
         return c
+
+
+def batch_configs() -> list[tuple[int, int, int]]:
+    n = C.c_uint32(0)
+    check(_L.ww_batch_configs(None, 0, C.byref(n)), "ww_batch_configs")
+    arr = (BatchCfg * n.value)()
+    check(_L.ww_batch_configs(arr, n.value, C.byref(n)), "ww_batch_configs")
+    return [c.as_tuple() for c in arr]
+
+
+def _units(ranges) -> C.Array:
+    arr = (Unit * max(len(ranges), 1))()
+    for i, (a, b) in enumerate(ranges):
+        arr[i].start, arr[i].end = a, b
+    return arr
+
+
+class Batch:
+    """The batched search on a Context: many ranges in one persistent launch."""
+
+    def __init__(self, ctx: Context, max_hits: int = 1 << 16):
+        self.ctx = ctx
+        check(_L.ww_batch_reserve_hits(ctx.h, max_hits), "ww_batch_reserve_hits")
+        self.max_hits = max_hits
+
+    def set_config(self, seg_words: int, threads: int, ppt: int) -> None:
+        c = BatchCfg(seg_words, threads, ppt, 0)
+        check(_L.ww_batch_set_config(self.ctx.h, C.byref(c)), "ww_batch_set_config")
+
+    def config(self) -> tuple[int, int, int]:
+        c = BatchCfg()
+        check(_L.ww_batch_get_config(self.ctx.h, C.byref(c)), "ww_batch_get_config")
+        return c.as_tuple()
+
+    def tune(self, sample) -> tuple[tuple[int, int, int], float]:
+        u = _units(sample)
+        best = BatchCfg()
+        ms = C.c_float(0)
+        check(_L.ww_batch_tune(self.ctx.h, u, len(sample), C.byref(best), C.byref(ms)), "ww_batch_tune")
+        return best.as_tuple(), float(ms.value)
+
+    def submit(self, ranges) -> None:
+        self._n = len(ranges)
+        self._u = _units(ranges)
+        check(_L.ww_batch_submit(self.ctx.h, self._u, self._n), "ww_batch_submit")
+
+    def collect(self) -> list[dict]:
+        out = (UnitResult * max(self._n, 1))()
+        hc = C.c_uint32(0)
+        check(_L.ww_batch_collect(self.ctx.h, out, self._n, C.byref(hc)), "ww_batch_collect")
+        self.hit_count = hc.value
+        return [dict(checksum=r.checksum, prp_count=r.prp_count, hits=r.hits, tiles_done=r.tiles_done)
+                for r in out[: self._n]]
+
+    def run(self, ranges) -> list[dict]:
+        self.submit(ranges)
+        return self.collect()
+
+    def hits(self) -> list[tuple[int, int, int, int, int]]:
+        cap = self.max_hits
+        arr = (Hit * cap)()
+        units = (C.c_uint32 * cap)()
+        n = C.c_uint32(0)
+        check(_L.ww_batch_hits(self.ctx.h, arr, units, cap, C.byref(n)), "ww_batch_hits")
+        return [(units[i], arr[i].p, arr[i].result, arr[i].rem, arr[i].quot) for i in range(min(n.value, cap))]
+
+
+class Server:
+    """Continuous-batching request server on a Context."""
+
+    def __init__(self, ctx: Context, prp_pool_bytes: int = 8 << 30, max_active: int = 64,
+                 epoch_tiles: int = 2048, max_hits: int = 1 << 15, store_prps: bool = True):
+        self.ctx = ctx
+        cfg = ServerCfg(prp_pool_bytes, max_active, epoch_tiles, max_hits, 1 if store_prps else 0)
+        check(_L.ww_server_open(ctx.h, C.byref(cfg)), "ww_server_open")
+        self.cap = max_active
+        self._buf = (RequestResult * max_active)()
+
+    def close(self):
+        if self.ctx and self.ctx.h:
+            _L.ww_server_close(self.ctx.h)
+        self.ctx = None
+
+    def submit(self, reqs) -> None:
+        arr = (Request * max(len(reqs), 1))()
+        for i, (rid, a, b) in enumerate(reqs):
+            arr[i].id, arr[i].start, arr[i].end = rid, a, b
+        check(_L.ww_server_submit(self.ctx.h, arr, len(reqs)), "ww_server_submit")
+
+    def step(self) -> list[dict]:
+        n = C.c_uint32(0)
+        check(_L.ww_server_step(self.ctx.h, self._buf, self.cap, C.byref(n)), "ww_server_step")
+        return [dict(id=r.id, checksum=r.checksum, prp_count=r.prp_count, prps_stored=r.prps_stored,
+                     hits=r.hits, status=r.status, t_submit=r.t_submit, t_admit=r.t_admit, t_done=r.t_done)
+                for r in self._buf[: n.value]]
+
+    def status(self) -> tuple[int, int, int]:
+        q, a, u = C.c_uint32(0), C.c_uint32(0), C.c_uint64(0)
+        check(_L.ww_server_status(self.ctx.h, C.byref(q), C.byref(a), C.byref(u)), "ww_server_status")
+        return q.value, a.value, u.value
+
+    def hits(self, rid: int) -> list[tuple[int, int, int, int]]:
+        cap = 4096
+        arr = (Hit * cap)()
+        n = C.c_uint32(0)
+        check(_L.ww_server_hits(self.ctx.h, rid, arr, cap, C.byref(n)), "ww_server_hits")
+        return [(arr[i].p, arr[i].result, arr[i].rem, arr[i].quot) for i in range(min(n.value, cap))]
+
+    def prps(self, rid: int, cap: int) -> np.ndarray:
+        out = np.zeros(max(cap, 1), dtype=np.uint64)
+        n = C.c_uint64(0)
+        check(_L.ww_server_prps(self.ctx.h, rid, out.ctypes.data, cap, C.byref(n)), "ww_server_prps")
+        return out[: min(n.value, cap)]
+
+    def drain(self, max_steps: int = 100000) -> list[dict]:
+        done = []
+        for _ in range(max_steps):
+            done += self.step()
+            q, a, _ = self.status()
+            if q == 0 and a == 0:
+                break
+        return done
+
+
+def uneven_units(seed: int, n: int, wmin: float = 1e6, wmax: float = 1e10, smin: int = 10**15,
+                 smax: int = 2**64 - 10**10, align: int = 30) -> list[tuple[int, int]]:
+    """The uneven-range mix: widths log-uniform in [wmin, wmax], starts
+    uniform in [smin, smax] rounded down to multiples of `align`."""
+    rng = np.random.default_rng(seed)
+    widths = np.exp(rng.uniform(np.log(wmin), np.log(wmax), n)).astype(np.float64)
+    starts = rng.integers(smin // align, smax // align, n, dtype=np.uint64, endpoint=False)
+    out = []
+    for s, w in zip(starts, widths):
+        a = int(s) * align
+        out.append((a, a + int(w)))
+    return out
 
 
 def digits(primes: np.ndarray, device: int = 0) -> np.ndarray:
