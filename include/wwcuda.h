@@ -293,6 +293,22 @@ int ww_parse_number(const char *text, uint64_t *out);
  * when buf is too small. */
 int ww_format_hits(ww_hit *hits, uint32_t n, char *buf, size_t cap, uint32_t *dropped);
 
+/* Checkpoint state (write_state / read_state, main.cpp:103-209): two files
+ * written alternately, each one line "start stop current cksm psum pcnt".
+ * ww_state_write writes the file due next (A when *write_a_next) and flips
+ * *write_a_next only when the file was closed successfully.
+ * ww_state_read returns 1 and the newer valid state (larger current; B on a
+ * tie) of the files whose start/stop match, 0 when neither is usable. */
+typedef struct {
+    uint64_t current, cksm;
+    double psum;
+    int32_t pcnt, pad;
+} ww_state;
+int ww_state_write(const char *file_a, const char *file_b, uint64_t start, uint64_t stop,
+                   const ww_state *st, int *write_a_next);
+int ww_state_read(const char *file_a, const char *file_b, uint64_t start, uint64_t stop, ww_state *st,
+                  int *write_a_next);
+
 /* Upper bound on the number of base-2 strong PRPs in [lo, hi) used to size
  * PRP buffers (replaces primesieve_count_primes, main.cpp:1087-1091). */
 uint64_t ww_prp_count_bound(uint64_t lo, uint64_t hi);

@@ -59,7 +59,7 @@ const std::vector<CfgEntry> &configs() {
         entry<4096, 128, 1>(),   entry<4096, 256, 1>(),   entry<4096, 512, 1>(),   entry<4096, 256, 2>(),
         entry<8192, 256, 1>(),   entry<8192, 512, 1>(),   entry<8192, 1024, 1>(),  entry<8192, 256, 2>(),
         entry<16384, 256, 1>(),  entry<16384, 512, 1>(),  entry<16384, 1024, 1>(), entry<16384, 512, 2>(),
-        entry<32768, 512, 1>(),  entry<32768, 1024, 1>(),
+        entry<32768, 256, 1>(),  entry<32768, 512, 1>(),
     };
     return table;
 }
@@ -180,6 +180,9 @@ BatchArgs make_args(BatchState &b, u32 n, u64 n_tiles) {
 }
 
 int launch_grid(const CfgEntry &e, int device, int *grid) {
+    int optin = 0;
+    WW_CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    if ((int)e.smem > optin) return set_err("batch config needs %zu bytes of shared memory", e.smem), WW_ERR_ARG;
     WW_CU(cudaFuncSetAttribute(e.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem));
     int per_sm = 0, sms = 0;
     WW_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, e.kernel, e.threads, e.smem));

@@ -6,6 +6,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <vector>
@@ -303,4 +304,73 @@ extern "C" int ww_selftest_candidates(uint64_t lo, uint64_t hi, uint64_t *out, u
     if (rescued) *rescued = rescue.size();
     for (u64 i = 0; i < cap && i < cand.size(); ++i) out[i] = cand[i];
     return WW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Checkpoint files (main.cpp:103-209).
+
+namespace {
+
+bool read_state_file(const char *name, uint64_t start, uint64_t stop, ww_state &st) {
+    FILE *in = fopen(name, "r");
+    if (!in) return false;
+    uint64_t a = 0, b = 0;
+    ww_state t{};
+    const int n = fscanf(in, "%" SCNu64 " %" SCNu64 " %" SCNu64 " %" SCNu64 " %lf %d", &a, &b, &t.current, &t.cksm,
+                         &t.psum, &t.pcnt);
+    fclose(in);
+    if (n != 6) {
+        fprintf(stderr, "Cannot parse %s !!!\n", name);
+        return false;
+    }
+    if (a != start || b != stop) return false;  // main.cpp:157,173
+    if (t.current < start || t.current > stop) return false;
+    st = t;
+    return true;
+}
+
+}  // namespace
+
+extern "C" int ww_state_write(const char *file_a, const char *file_b, uint64_t start, uint64_t stop,
+                              const ww_state *st, int *write_a_next) {
+    if (!file_a || !file_b || !st || !write_a_next) return WW_ERR_ARG;
+    const char *name = *write_a_next ? file_a : file_b;
+    FILE *out = fopen(name, "w");
+    if (!out) {
+        set_err("cannot open %s", name);
+        return WW_ERR_ARG;
+    }
+    if (fprintf(out, "%" PRIu64 " %" PRIu64 " %" PRIu64 " %" PRIu64 " %lf %d\n", start, stop, st->current, st->cksm,
+                st->psum, st->pcnt) < 0) {
+        fclose(out);
+        set_err("cannot write %s", name);
+        return WW_ERR_ARG;
+    }
+    fflush(out);
+    fsync(fileno(out));
+    if (fclose(out) == 0) *write_a_next = !*write_a_next;  // main.cpp:124-129
+    return WW_OK;
+}
+
+extern "C" int ww_state_read(const char *file_a, const char *file_b, uint64_t start, uint64_t stop, ww_state *st,
+                             int *write_a_next) {
+    if (!file_a || !file_b || !st || !write_a_next) return WW_ERR_ARG;
+    ww_state a{}, b{};
+    bool ga = read_state_file(file_a, start, stop, a);
+    bool gb = read_state_file(file_b, start, stop, b);
+    if (ga && gb) {  // main.cpp:179-185
+        if (a.current > b.current) gb = false;
+        else ga = false;
+    }
+    if (ga) {
+        *st = a;
+        *write_a_next = 0;
+        return 1;
+    }
+    if (gb) {
+        *st = b;
+        *write_a_next = 1;
+        return 1;
+    }
+    return 0;
 }

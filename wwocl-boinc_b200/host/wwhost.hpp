@@ -33,65 +33,26 @@ struct State {
     int pcnt = 0;
 };
 
-// write_state (main.cpp:103-130): write the file due next; switch to the
-// other one only when the close succeeded, so a torn write leaves the older
-// file intact.
+// write_state / read_state (main.cpp:103-209) live in the library
+// (ww_state_write / ww_state_read) so the CPU tests can exercise them.
 inline void write_state(const Files &f, uint64_t start, uint64_t stop, const State &s, bool &write_a_next) {
-    const std::string &name = write_a_next ? f.state_a : f.state_b;
-    FILE *out = fopen(name.c_str(), "w");
-    if (!out) {
-        fprintf(stderr, "Cannot open %s !!!\n", name.c_str());
-        return;
-    }
-    if (fprintf(out, "%" PRIu64 " %" PRIu64 " %" PRIu64 " %" PRIu64 " %lf %d\n", start, stop, s.current, s.cksm,
-                s.psum, s.pcnt) < 0) {
-        fprintf(stderr, "Cannot write to %s !!! Continuing...\n", name.c_str());
-        fclose(out);
-        return;
-    }
-    fflush(out);
-    fsync(fileno(out));
-    if (fclose(out) == 0) write_a_next = !write_a_next;
+    ww_state st{s.current, s.cksm, s.psum, s.pcnt, 0};
+    int a = write_a_next ? 1 : 0;
+    if (ww_state_write(f.state_a.c_str(), f.state_b.c_str(), start, stop, &st, &a) != WW_OK)
+        fprintf(stderr, "Cannot write state !!! Continuing... (%s)\n", ww_last_error());
+    write_a_next = a != 0;
 }
 
-inline bool read_one(const std::string &name, uint64_t start, uint64_t stop, State &s) {
-    FILE *in = fopen(name.c_str(), "r");
-    if (!in) return false;
-    uint64_t a = 0, b = 0;
-    State t;
-    const int n = fscanf(in, "%" SCNu64 " %" SCNu64 " %" SCNu64 " %" SCNu64 " %lf %d", &a, &b, &t.current, &t.cksm,
-                         &t.psum, &t.pcnt);
-    fclose(in);
-    if (n != 6) {
-        fprintf(stderr, "Cannot parse %s !!!\n", name.c_str());
-        return false;
-    }
-    if (a != start || b != stop) return false;  // main.cpp:157,173
-    s = t;
-    return true;
-}
-
-// read_state (main.cpp:136-209): the newer valid file wins (larger current;
-// B on a tie, as the reference's `current_a > current_b` test gives).
 inline bool read_state(const Files &f, uint64_t start, uint64_t stop, State &s, bool &write_a_next) {
-    State a, b;
-    bool ga = read_one(f.state_a, start, stop, a);
-    bool gb = read_one(f.state_b, start, stop, b);
-    if (ga && gb) {
-        if (a.current > b.current) gb = false;
-        else ga = false;
-    }
-    if (ga) {
-        s = a;
-        write_a_next = false;
-        return true;
-    }
-    if (gb) {
-        s = b;
-        write_a_next = true;
-        return true;
-    }
-    return false;
+    ww_state st{};
+    int a = 1;
+    if (ww_state_read(f.state_a.c_str(), f.state_b.c_str(), start, stop, &st, &a) != 1) return false;
+    s.current = st.current;
+    s.cksm = st.cksm;
+    s.psum = st.psum;
+    s.pcnt = st.pcnt;
+    write_a_next = a != 0;
+    return true;
 }
 
 // report_solution (main.cpp:741-765): append and fsync.  Returns false on

@@ -84,6 +84,11 @@ class ServerCfg(C.Structure):
                 ("max_hits", C.c_uint32), ("store_prps", C.c_uint32)]
 
 
+class State(C.Structure):
+    _fields_ = [("current", C.c_uint64), ("cksm", C.c_uint64), ("psum", C.c_double), ("pcnt", C.c_int32),
+                ("pad", C.c_int32)]
+
+
 _U64P = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 _VP = C.c_void_p
 _SIGS = {
@@ -123,6 +128,10 @@ _SIGS = {
     "ww_format_hits": (C.c_int, [C.POINTER(Hit), C.c_uint32, C.c_char_p, C.c_size_t,
                                  C.POINTER(C.c_uint32)]),
     "ww_prp_count_bound": (C.c_uint64, [C.c_uint64, C.c_uint64]),
+    "ww_state_write": (C.c_int, [C.c_char_p, C.c_char_p, C.c_uint64, C.c_uint64, C.POINTER(State),
+                                 C.POINTER(C.c_int)]),
+    "ww_state_read": (C.c_int, [C.c_char_p, C.c_char_p, C.c_uint64, C.c_uint64, C.POINTER(State),
+                                C.POINTER(C.c_int)]),
     "ww_selftest_digits": (C.c_int, [_U64P, C.c_uint64, _U64P]),
     "ww_selftest_range": (C.c_int, [C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64),
                                     C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
@@ -197,6 +206,26 @@ def format_hits(hits: list[tuple[int, int, int, int]]) -> tuple[str, int]:
     dropped = C.c_uint32(0)
     check(_L.ww_format_hits(arr, len(hits), buf, len(buf), C.byref(dropped)), "ww_format_hits")
     return buf.value.decode(), int(dropped.value)
+
+
+def state_write(file_a: str, file_b: str, start: int, stop: int, current: int, cksm: int, psum: float,
+                pcnt: int, write_a_next: bool) -> bool:
+    st = State(current, cksm, psum, pcnt, 0)
+    a = C.c_int(1 if write_a_next else 0)
+    check(_L.ww_state_write(file_a.encode(), file_b.encode(), start, stop, C.byref(st), C.byref(a)),
+          "ww_state_write")
+    return bool(a.value)
+
+
+def state_read(file_a: str, file_b: str, start: int, stop: int):
+    """(state dict, write_a_next) or None."""
+    st = State()
+    a = C.c_int(1)
+    rc = check(_L.ww_state_read(file_a.encode(), file_b.encode(), start, stop, C.byref(st), C.byref(a)),
+               "ww_state_read")
+    if rc != 1:
+        return None
+    return dict(current=st.current, cksm=st.cksm, psum=st.psum, pcnt=st.pcnt), bool(a.value)
 
 
 def prp_count_bound(lo: int, hi: int) -> int:
