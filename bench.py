@@ -189,7 +189,7 @@ def run_batched_vs_plain(ww, local: int, n_units: int, tune_units: int = 32):
     the tile queue after the autotuner picked the configuration.  Per-unit
     checksums and PRP counts must agree."""
     units = ww.uneven_units(11, 4096)[:n_units]
-    ctx = ww.Context(local, max_prps=1 << 24, max_hits=15000)
+    ctx = ww.Context(local, max_prps=ww.prp_count_bound(0, 1 << 30), max_hits=15000)
     b = ww.Batch(ctx)
     cfg, _ = b.tune(units[:tune_units])
     b.run(units)  # warm
@@ -199,17 +199,49 @@ def run_batched_vs_plain(ww, local: int, n_units: int, tune_units: int = 32):
     ctx.sync()
     batch_ms = ctx.elapsed_ms(0, 1)
     prps = sum(r["prp_count"] for r in res)
+    # plain, config 3's definition: per range, sieve -> Wieferich -> WSS kernels
+    # with a checkpoint (sync, counters and hits read back, clear) every 2^30
+    # numbers and at the range's end
+    ckpt = 1 << 30
+    t0 = time.perf_counter()
+    plain = []
+    for a, z in units:
+        cks, cnt, hits = 0, 0, 0
+        start = a
+        ctx.clear_results()
+        while start < z:
+            stop = min(start + ckpt, z)
+            ctx.clear_segment()
+            ctx.sieve_prp(start, stop)
+            ctx.wieferich()
+            ctx.wallsunsun()
+            ctx.sync()
+            k = ctx.counters()
+            if k["result_count"]:
+                ctx.hits()
+            cks, cnt, hits = (cks + k["checksum"]) % 2**64, cnt + k["total_prp_count"], hits + k["result_count"]
+            ctx.clear_results()
+            start = stop
+        plain.append((cks, cnt, hits))
+    plain_s = time.perf_counter() - t0
+    # the same ranges one per launch sequence with the fused test kernel
     t0 = time.perf_counter()
     alone = [ctx.run_range(a, z) for a, z in units]
-    plain_s = time.perf_counter() - t0
+    fused_s = time.perf_counter() - t0
     equal = all(r["checksum"] == a["checksum"] and r["prp_count"] == a["total_prp_count"] and
-                r["hits"] == a["result_count"] for r, a in zip(res, alone))
+                r["hits"] == a["result_count"] and (r["checksum"], r["prp_count"], r["hits"]) == p
+                for r, a, p in zip(res, alone, plain))
     ctx.close()
     numbers = sum(z - a for a, z in units)
     return {"workload": f"first {n_units} units of the seed-11 uneven mix (config 4)", "units": n_units,
             "numbers": numbers, "prps": prps, "batched_primes_per_s": prps / (batch_ms * 1e-3),
-            "plain_primes_per_s": prps / plain_s, "batched_numbers_per_s": numbers / (batch_ms * 1e-3),
-            "speedup_batched_vs_plain": plain_s / (batch_ms * 1e-3), "per_unit_bit_identical": bool(equal),
+            "plain_primes_per_s": prps / plain_s, "plain_fused_primes_per_s": prps / fused_s,
+            "batched_numbers_per_s": numbers / (batch_ms * 1e-3),
+            "speedup_batched_vs_plain": plain_s / (batch_ms * 1e-3),
+            "speedup_batched_vs_plain_fused": fused_s / (batch_ms * 1e-3),
+            "plain_definition": "per range: sieve, Wieferich, WSS kernels; checkpoint sync + read-back "
+                                "every 2^30 numbers (config 3)",
+            "per_unit_bit_identical": bool(equal),
             "tuned_config": {"seg_words": cfg[0], "seg_bytes": 4 * cfg[0], "threads": cfg[1],
                              "primes_per_thread": cfg[2]}}
 

@@ -225,8 +225,11 @@ __global__ void __launch_bounds__(Cfg::kThreads) k_tiles(BatchArgs a) {
         const u64 nbase = b0 + 1;
         deep_collect(nbase, (u32)nvalid, bitmap, rescue, &s_rescue_n, threadIdx.x, Cfg::kThreads);
         __syncthreads();
-        const u32 nresc = s_rescue_n <= (u32)kRescueCap ? s_rescue_n : 0u;
-        if (s_rescue_n <= (u32)kRescueCap) deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, Cfg::kThreads);
+        if (s_rescue_n <= (u32)kRescueCap) {  // else: this tile keeps the small-prime sieve only
+            deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, Cfg::kThreads);
+            __syncthreads();
+            deep_unmark(bitmap, rescue, s_rescue_n, threadIdx.x, Cfg::kThreads);
+        }
         __syncthreads();
 
         // ---- chunks of 32 words, taken dynamically by the warps
@@ -262,11 +265,6 @@ __global__ void __launch_bounds__(Cfg::kThreads) k_tiles(BatchArgs a) {
                 __syncwarp();
             }
         };
-        // this warp's share of the rescue list
-        for (u32 base = warp * 32; base < nresc; base += Cfg::kWarps * 32) {
-            const bool act = base + lane < nresc;
-            sprp_step(act ? rescue[base + lane] : 0u, act);
-        }
         for (;;) {
             u32 chunk = 0;
             if (lane == 0) chunk = atomicAdd(&s_chunk, 1u);

@@ -125,7 +125,12 @@ int ww_launch_getsegprimes(uint64_t low, uint64_t high, int32_t wheelidx, uint64
     const uint64_t span = high - b0;
     const uint64_t per = 2ull * kSegOdd;
     const uint64_t nseg = span / per + (span % per ? 1 : 0);
-    const uint64_t grid = nseg < (uint64_t)sm_count() * 6 ? nseg : (uint64_t)sm_count() * 6;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sieve_prp, kSieveThreads, 0) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    const uint64_t slots = (uint64_t)sm_count() * (uint64_t)per_sm;
+    const uint64_t grid = nseg < slots ? nseg : slots;
     PrpOut out{(u64 *)g_prime, (u64 *)g_invert, primecount, capacity, overflow};
     k_sieve_prp<<<(unsigned)grid, kSieveThreads, 0, as_stream(stream)>>>(low, high, nseg, out);
     WW_CHECK_LAUNCH();

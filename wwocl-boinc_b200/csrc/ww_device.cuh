@@ -16,7 +16,6 @@ constexpr int kSegOdd = kSegWords * 32;       // odd numbers per segment
 constexpr int kSieveThreads = 256;
 constexpr int kSieveWarps = kSieveThreads / 32;
 constexpr int kWordsPerThread = kSegWords / kSieveThreads;
-constexpr int kWordsPerWarp = kSegWords / kSieveWarps;
 constexpr int kQueueCap = 640;  // 31 carried + 32 words x at most 18 survivors
 constexpr int kTestThreads = 256;
 #ifndef WW_TEST_MINB
@@ -105,6 +104,17 @@ __device__ __forceinline__ void deep_collect(u64 first, u32 nvalid, const u32 *b
                 if (k < kRescueCap) rescue[k] = j;
             }
         }
+    }
+}
+
+// Clear the rescued bits again once the deep marking is complete, so they
+// reach the PRP test through the bitmap like any survivor.  A number in two
+// rescue classes (a pseudoprime with two deep factors) is listed twice and
+// cleared twice: it is still tested once.
+__device__ __forceinline__ void deep_unmark(u32 *bitmap, const u32 *rescue, u32 nresc, int tid, int nthreads) {
+    for (u32 i = tid; i < nresc; i += nthreads) {
+        const u32 j = rescue[i];
+        atomicAnd(&bitmap[j >> 5], ~(1u << (j & 31)));
     }
 }
 

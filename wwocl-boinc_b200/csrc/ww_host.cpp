@@ -295,11 +295,10 @@ extern "C" int ww_selftest_candidates(uint64_t lo, uint64_t hi, uint64_t *out, u
         const u32 *e = kDeepHost[i];
         for (u64 j = deep_first_multiple(first, e[0], e[2]); j < nvalid; j += e[0]) mark(j);
     }
+    for (u64 j : rescue) bitmap[j >> 5] &= ~(1u << (j & 31));  // as deep_unmark does
     std::vector<u64> cand;
     for (u64 j = 0; j < nvalid; ++j)
         if (!marked(j)) cand.push_back(first + 2 * j);
-    for (u64 j : rescue) cand.push_back(first + 2 * j);
-    std::sort(cand.begin(), cand.end());
     *n = cand.size();
     if (rescued) *rescued = rescue.size();
     for (u64 i = 0; i < cap && i < cand.size(); ++i) out[i] = cand[i];

@@ -24,7 +24,7 @@ __global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64
     __shared__ u32 bitmap[kSegWords];
     __shared__ u32 queue[kSieveWarps][kQueueCap];
     __shared__ u32 rescue[kRescueCap];
-    __shared__ u32 rescue_n;
+    __shared__ u32 rescue_n, s_chunk;
     const u64 b0 = lo & ~1ull;
     const u64 span = hi - b0;
     const int lane = threadIdx.x & 31;
@@ -57,56 +57,62 @@ __global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64
                 bitmap[w] = m;
             }
         }
-        if (threadIdx.x == 0) rescue_n = 0;
+        if (threadIdx.x == 0) {
+            rescue_n = 0;
+            s_chunk = 0;
+        }
         __syncthreads();
 
         // ---- deep sieve 127..2^16 with the pseudoprime rescue list
         const u64 nbase = b0 + seg_off + 1;
         deep_collect(nbase, (u32)nvalid, bitmap, rescue, &rescue_n, threadIdx.x, kSieveThreads);
         __syncthreads();
-        const u32 nresc = rescue_n <= (u32)kRescueCap ? rescue_n : 0u;
-        if (rescue_n <= (u32)kRescueCap) deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, kSieveThreads);
-        __syncthreads();
-        for (u32 base = warp * 32; base < nresc; base += kSieveWarps * 32) {
-            const bool act = base + lane < nresc;
-            const u32 j = act ? rescue[base + lane] : 0u;
-            sprp_emit(out, nbase + 2ull * j, act);
+        if (rescue_n <= (u32)kRescueCap) {  // else: this segment keeps the small-prime sieve only
+            deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, kSieveThreads);
+            __syncthreads();
+            deep_unmark(bitmap, rescue, rescue_n, threadIdx.x, kSieveThreads);
         }
+        __syncthreads();
 
-        // ---- per-warp compaction + SPRP, 32 candidates at a time
+        // ---- warps take 32-word chunks dynamically (so they reach the next
+        // barrier together), compact the survivors with ballot/popc into a
+        // warp queue and PRP-test them 32 at a time
         u32 *q = queue[warp];
         int qn = 0;
-        for (int wb = warp * kWordsPerWarp; wb < (warp + 1) * kWordsPerWarp; wb += 32) {
-            const int w = wb + lane;
-            u32 cand = ~bitmap[w];
-            const int cnt = __popc(cand);
-            int incl = cnt;
+        for (;;) {
+            u32 chunk = 0;
+            if (lane == 0) chunk = atomicAdd(&s_chunk, 1u);
+            chunk = __shfl_sync(0xffffffffu, chunk, 0);
+            const bool more = chunk < (u32)(kSegWords / 32);
+            if (more) {
+                const int w = chunk * 32 + lane;
+                u32 cand = ~bitmap[w];
+                const int cnt = __popc(cand);
+                int incl = cnt;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
-            }
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            int pos = qn + incl - cnt;
-            while (cand) {
-                const int b = __ffs(cand) - 1;
-                q[pos++] = (u32)(w * 32 + b);
-                cand &= cand - 1;
-            }
-            qn += total;
-            __syncwarp();
-            while (qn >= 32) {
-                qn -= 32;
-                const u32 j = q[qn + lane];
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                int pos = qn + incl - cnt;
+                while (cand) {
+                    const int b = __ffs(cand) - 1;
+                    q[pos++] = (u32)(w * 32 + b);
+                    cand &= cand - 1;
+                }
+                qn += total;
                 __syncwarp();
-                sprp_emit(out, nbase + 2ull * j, true);
             }
-            __syncwarp();
-        }
-        if (qn > 0) {
-            const bool act = lane < qn;
-            const u32 j = act ? q[lane] : 0u;
-            sprp_emit(out, nbase + 2ull * j, act);
+            while (qn >= 32 || (!more && qn > 0)) {
+                const int take = qn >= 32 ? 32 : qn;
+                qn -= take;
+                const bool act = lane < take;
+                const u32 j = act ? q[qn + lane] : 0u;
+                __syncwarp();
+                sprp_emit(out, nbase + 2ull * j, act);
+            }
+            if (!more) break;
         }
         __syncthreads();  // bitmap reused by the next segment
     }
