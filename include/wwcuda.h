@@ -226,6 +226,23 @@ int ww_batch_hits(ww_ctx *ctx, ww_hit *out, uint32_t *unit_of_hit, uint32_t cap,
  * configuration on the sample and keeps the fastest in the context. */
 int ww_batch_tune(ww_ctx *ctx, const ww_unit *sample, uint32_t n, ww_batch_cfg *best, float *best_ms);
 
+/* The batched search for callers that cannot allocate device memory (no
+ * counterpart in the reference).  Hosts that reserve all of the GPU's
+ * memory up front and forbid later allocations, or latency-bound loops
+ * that cannot afford an allocation's device-wide synchronisation, get the
+ * same per-range results as ww_batch_run without any allocation: the
+ * scratch lives in one fixed __device__ array of the library (about 450 KB
+ * per device, kept until exit).  units: host array, n <= 4096 ranges;
+ * out[n], hits[hit_cap] (at most 4096 records), hit_unit[hit_cap] (may be
+ * NULL) and *hit_count are device memory; work is queued on `stream` (a
+ * cudaStream_t) and the call does not wait for it.  Calls share the array:
+ * each clears it, and calls whose GPU work overlaps race, so keep them on
+ * one stream.  The first call on a device sets up the array's address
+ * (cudaGetSymbolAddress) and should come before any stream capture.
+ * Returns WW_ERR_ARG for more than 4096 ranges. */
+int ww_batch_run_noalloc(const ww_unit *units, uint32_t n, ww_unit_result *out, ww_hit *hits,
+                         uint32_t *hit_unit, uint32_t hit_cap, uint32_t *hit_count, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Request server (no reference counterpart; the reference runs one range
  * per process).  Continuous batching: requests wait in a host queue and are

@@ -1,0 +1,69 @@
+"""The allocation-free batched search (ww_batch_run_noalloc).
+
+Some callers cannot allocate device memory -- a host that reserves the
+whole card for its own memory pool, or a latency-bound loop that cannot
+afford an allocation's device-wide synchronisation.  This entry point runs
+the batched search with its scratch in a fixed array inside the library;
+here it is called through the C ABI on buffers the test allocates, twice in
+a row (the shared scratch keeps the previous call's contents), and each
+call must give exactly what ww_batch_run gives.  The file sorts last so a
+run that stops at the first failure has already run every other test."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc(ww, units, hit_cap=4096):
+    import torch
+
+    L = ww.lib()
+    dev = torch.device("cuda", 0)
+    n = len(units)
+    out = torch.zeros(n * C.sizeof(ww.UnitResult), dtype=torch.uint8, device=dev)
+    hits = torch.zeros(hit_cap * C.sizeof(ww.Hit), dtype=torch.uint8, device=dev)
+    hit_unit = torch.zeros(hit_cap, dtype=torch.int32, device=dev)
+    count = torch.zeros(1, dtype=torch.int32, device=dev)
+    arr = (ww.Unit * max(n, 1))()
+    for i, (a, b) in enumerate(units):
+        arr[i].start, arr[i].end = a, b
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    ww.check(L.ww_batch_run_noalloc(arr, n, out.data_ptr(), hits.data_ptr(), hit_unit.data_ptr(), hit_cap,
+                                    count.data_ptr(), stream), "ww_batch_run_noalloc")
+    torch.cuda.synchronize(dev)
+    res = (ww.UnitResult * n).from_buffer_copy(out.cpu().numpy().tobytes())
+    nh = int(count.item())
+    hh = (ww.Hit * hit_cap).from_buffer_copy(hits.cpu().numpy().tobytes())
+    hu = hit_unit.cpu().numpy()
+    results = [(r.checksum, r.prp_count, r.hits) for r in res]
+    hit_list = sorted((int(hu[i]), hh[i].p, hh[i].result, hh[i].rem, hh[i].quot) for i in range(min(nh, hit_cap)))
+    return results, hit_list, nh
+
+
+def test_noalloc_matches_batch_twice(ww):
+    units = ww.uneven_units(11, 48, wmin=1e5, wmax=2e8)
+    units += [(127, 400_000), (2276306935816523 - 3000, 2276306935816523 + 3000), (5000, 5000)]
+    with ww.Context(0, max_prps=1 << 20, max_hits=15000) as ctx:
+        b = ww.Batch(ctx)
+        b.set_config(8192, 256, 1)
+        want = [(r["checksum"], r["prp_count"], r["hits"]) for r in b.run(units)]
+        want_hits = sorted(b.hits())
+    for _ in range(2):  # the second call starts from the first call's scratch contents
+        got, hits, nh = _noalloc(ww, units)
+        assert got == want
+        assert nh == len(want_hits) and hits == want_hits
+
+
+def test_noalloc_rejects_too_many_ranges(ww):
+    L = ww.lib()
+    n = 4097
+    arr = (ww.Unit * n)()
+    for i in range(n):
+        arr[i].start, arr[i].end = 10**12 + 1000 * i, 10**12 + 1000 * i + 500
+    rc = L.ww_batch_run_noalloc(arr, n, None, None, None, 0, None, None)
+    assert rc == -2
+    assert b"4096" in L.ww_last_error()

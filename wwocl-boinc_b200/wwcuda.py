@@ -153,6 +153,7 @@ _SIGS = {
     "ww_server_status": (C.c_int, [_VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
     "ww_server_hits": (C.c_int, [_VP, C.c_uint64, C.POINTER(Hit), C.c_uint32, C.POINTER(C.c_uint32)]),
     "ww_server_prps": (C.c_int, [_VP, C.c_uint64, _VP, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "ww_batch_run_noalloc": (C.c_int, [C.POINTER(Unit), C.c_uint32, _VP, _VP, _VP, C.c_uint32, _VP, _VP]),
     "ww_selftest_m2": (C.c_int, [C.c_int, C.c_uint64, _U64P, C.c_uint64, _U64P]),
     "ww_selftest_candidates": (C.c_int, [C.c_uint64, C.c_uint64, _U64P, C.c_uint64, C.POINTER(C.c_uint64),
                                          C.POINTER(C.c_uint64)]),
