@@ -405,7 +405,7 @@ def main():
                 "frac": achieved / imad_peak, "traffic": profile_traffic(),
                 "peak_source": "measured live: mad.lo.u32 chains on every SM (ww_pipe_bench mode 0)",
                 "ops_per_prime": per_prime,
-                "hbm": {"bytes_per_launch": 8 * n, "GBps": 8 * n / (launch_ms * 1e-3) / 1e9,
+                "hbm": {"bytes_per_launch": 16 * n, "GBps": 16 * n / (launch_ms * 1e-3) / 1e9,
                         "peak_GBps": json.loads(PEAKS.read_text())["hbm_gbs"] if PEAKS.exists() else 6650.0}}
 
     cpu = None
