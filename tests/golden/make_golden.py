@@ -5,11 +5,14 @@ are mounted:
 
     make -C oracle && python tests/golden/make_golden.py
 
+    python tests/golden/make_golden.py --long    # config 3's range, minutes
+
 Outputs (small, committed):
   ref_ranges.json  per-range PRP count, checksum and CPU result count
   ref_terms.npz    per-prime low 32 bits of the Wieferich and WSS checksum
                    terms and the wwcpu.cpp hit flags for fixed prime samples
   ref_prps.json    PRP-list digests (count, sum, sha256 of the sorted list)
+  ref_long.json    config 3's full range (with --long)
 """
 from __future__ import annotations
 
@@ -114,10 +117,26 @@ def parse_tests_txt(path: Path) -> list[dict]:
     return cases
 
 
+def long_ranges(ref: RefCPU) -> None:
+    """Config 3's range [2^64-2^35, 2^64-2^35+2^34): about 3.9e8 PRPs, several
+    minutes on 8 cores (only with --long)."""
+    lo = 2**64 - 2**35
+    hi = lo + 2**34
+    r = ref.scan_range(lo, hi, nthreads=8)
+    out = {"config3": {"lo": lo, "hi": hi, "prp_count": r["prp_count"], "checksum": "%016X" % r["checksum"],
+                       "cpu_results": r["cpu_results"]}}
+    (OUT / "ref_long.json").write_text(json.dumps(out, indent=1) + "\n")
+    print(out, flush=True)
+
+
 def main() -> None:
     ref = RefCPU()
     o = Oracle()
-    ref_tree = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    if "--long" in sys.argv:
+        long_ranges(ref)
+        return
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    ref_tree = Path(args[0]) if args else Path("/root/reference")
     cases = parse_tests_txt(ref_tree / "tests.txt")
     (OUT / "tests_txt.json").write_text(json.dumps(cases, indent=1) + "\n")
     print(cases, flush=True)

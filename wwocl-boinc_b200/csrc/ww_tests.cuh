@@ -81,10 +81,9 @@ WW_HD D2 wieferich_digits_t(u64 p, u64 q, D2 one) {
 
 // F_{p-(p|5)} mod p^2 as canonical digits.  The reference walks the
 // (F_k, F_{k-1}) doubling ladder, two squarings and a product per bit
-// (wallsunsun.cl:242-300).  Here the Lucas numbers V_k = L_k run a
-// Montgomery ladder (V_k, V_{k+1}), one squaring and one product per bit:
-//   V_2k = V_k^2 - 2(-1)^k,  V_2k+1 = V_k V_k+1 - (-1)^k,
-//   V_2k+2 = V_k+1^2 + 2(-1)^k,
+// (wallsunsun.cl:242-300).  Here the Lucas numbers V_k = L_k run a ladder
+// on (V_k, V_{k+1}) with two squarings per bit:
+//   V_2k = V_k^2 - 2(-1)^k,  V_2k+2 = V_k+1^2 + 2(-1)^k,  V_2k+1 = V_2k+2 - V_2k,
 // and F_n = (2 V_{n+1} - V_n) / 5 gives the same residue exactly (5 is a
 // unit mod p^2 since p has no factor below 127).
 template <class A>
@@ -94,19 +93,18 @@ WW_HD D2 wss_digits_t(u64 p, u64 q, D2 one) {
     const u64 n = (pm5 == 2 || pm5 == 3) ? p + 1 : p - 1;  // p - (p|5)
     const D2 zero = {0, 0};
     const D2 two = m2_dbl(one, p);
-    const D2 mone = m2_sub(zero, one, p);
     const D2 mtwo = m2_sub(zero, two, p);
     D2 a = one;                  // V_1
     D2 b = m2_add(two, one, p);  // V_2
     bool odd = true;             // parity of the ladder index k
     for (int i = top_bit(n) - 1; i >= 0; --i) {
         const bool bit = (n >> i) & 1;
-        const D2 sq = ar.sqr(sel(bit, b, a));
-        const D2 pr = ar.mul(a, b);
-        const D2 np = m2_add(pr, sel(odd, one, mone), p);             // V_k V_k+1 - (-1)^k
-        const D2 ns = m2_add(sq, sel(bit ^ odd, two, mtwo), p);       // V^2 -/+ 2(-1)^k
-        a = sel(bit, np, ns);
-        b = sel(bit, ns, np);
+        const D2 c = sel(odd, two, mtwo);  // -2(-1)^k
+        const D2 v2k = m2_add(ar.sqr(a), c, p);
+        const D2 v2k2 = m2_sub(ar.sqr(b), c, p);
+        const D2 v2k1 = m2_sub(v2k2, v2k, p);
+        a = sel(bit, v2k1, v2k);
+        b = sel(bit, v2k2, v2k1);
         odd = bit;
     }
     const D2 t = ar.redc(m2_sub(m2_dbl(b, p), a, p));
@@ -114,9 +112,13 @@ WW_HD D2 wss_digits_t(u64 p, u64 q, D2 one) {
 }
 
 // Both tests in one loop: each iteration advances the Lucas ladder by one
-// bit of p - (p|5) and the Wieferich powering by one bit of (p-1)/2, so the
-// three products of an iteration are independent and overlap in the pipe.
-// The Lucas exponent is one or two bits longer; its first steps run alone.
+// bit of p - (p|5) and the Wieferich powering by one bit of (p-1)/2.  The
+// ladder step uses two squarings instead of a squaring and a product:
+//   V_2k = V_k^2 - 2(-1)^k,  V_2k+2 = V_k+1^2 + 2(-1)^k,
+//   V_2k+1 = V_2k+2 - V_2k   (the recurrence V_m+1 = V_m + V_m-1),
+// so the three products of an iteration are squarings, independent of each
+// other, and no operand has to be selected before multiplying.  The Lucas
+// exponent is one or two bits longer; its first steps run alone.
 template <class A>
 WW_HD void both_digits_t(u64 p, u64 q, D2 one, D2 &s_out, D2 &c_out) {
     const A ar(p, q);
@@ -126,23 +128,24 @@ WW_HD void both_digits_t(u64 p, u64 q, D2 one, D2 &s_out, D2 &c_out) {
     const int top_e = top_bit(e);
     const D2 zero = {0, 0};
     const D2 two = m2_dbl(one, p);
-    const D2 mone = m2_sub(zero, one, p);
     const D2 mtwo = m2_sub(zero, two, p);
-    D2 a = one, b = m2_add(two, one, p);
+    D2 a = one, b = m2_add(two, one, p);  // V_1, V_2
     D2 w = two;
-    bool odd = true;
+    bool odd = true;  // parity of the ladder index k
     for (int i = top_bit(n) - 1; i >= 0; --i) {
         const bool bit = (n >> i) & 1;
-        const D2 sq = ar.sqr(sel(bit, b, a));
-        const D2 pr = ar.mul(a, b);
+        const D2 a2 = ar.sqr(a);
+        const D2 b2 = ar.sqr(b);
         if (i < top_e) {
             w = ar.sqr(w);
             w = sel((e >> i) & 1, m2_dbl(w, p), w);
         }
-        const D2 np = m2_add(pr, sel(odd, one, mone), p);
-        const D2 ns = m2_add(sq, sel(bit ^ odd, two, mtwo), p);
-        a = sel(bit, np, ns);
-        b = sel(bit, ns, np);
+        const D2 c = sel(odd, two, mtwo);     // -2(-1)^k
+        const D2 v2k = m2_add(a2, c, p);      // V_2k
+        const D2 v2k2 = m2_sub(b2, c, p);     // V_2k+2
+        const D2 v2k1 = m2_sub(v2k2, v2k, p); // V_2k+1
+        a = sel(bit, v2k1, v2k);
+        b = sel(bit, v2k2, v2k1);
         odd = bit;
     }
     s_out = ar.redc(w);
