@@ -44,9 +44,13 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n-primes", type=int, default=N_PRIMES)
-    ap.add_argument("--cpu-sample", type=int, default=1 << 20,
-                    help="primes in the bounded CPU-baseline sample")
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="primes in the bounded CPU sample (0: sized to --cpu-seconds)")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0,
+                    help="target wall time of the CPU-baseline sample (reference arm: per step / 8)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--range-width", type=float, default=float(1 << 34),
+                    help="width of the plain-path range leg starting at 2^64-2^35 (0: skip)")
     ap.add_argument("--batch-units", type=int, default=128,
                     help="units of the uneven mix for the batched-vs-plain line (0: skip)")
     ap.add_argument("--serve-seconds", type=float, default=10.0,
@@ -68,16 +72,22 @@ def config(args, world):
             "l2": "inputs larger than L2 (8 B x 2^26 = 512 MiB list per step)"}
 
 
-def algorithmic_imad_per_prime(primes: np.ndarray) -> float:
-    """32-bit multiply-adds one prime needs in the algorithm the kernel runs,
-    counted with the survey's fixed costs: a 64x64->128 product = 8, a low
-    64-bit product = 4, a high 64-bit product = 8; so a two-digit square
-    mod p^2 = 40 and a product = 48.  With k = bitlength(p): Wieferich does
-    k-2 squarings, the Lucas ladder k-1 (square + product), plus two
-    conversions out of Montgomery form (24 each)."""
+def algorithmic_imad_per_prime(primes: np.ndarray) -> tuple[float, float]:
+    """32-bit multiply instructions per prime, counted with fixed costs: a
+    64x64->128 product = 8, a low 64-bit product = 4, a high 64-bit product =
+    8, so a two-digit square mod p^2 = 40 and a product = 48.  k = bitlength(p).
+
+    Returns (reference_count, executed_count):
+      reference_count: the reference kernels' algorithm -- Wieferich k-3
+        squarings (wieferich.cl:196-328), the Lucas ladder k-1 steps of two
+        squarings and one product (wallsunsun.cl:221-354): 40(k-3) + 128(k-1).
+      executed_count: what k_test_prps runs -- Wieferich k-2 squarings, the
+        Lucas ladder k-1 steps of two squarings, two conversions out of
+        Montgomery form (24 each): 40(k-2) + 80(k-1) + 48."""
     bits = np.floor(np.log2(primes.astype(np.float64))) + 1  # exact away from powers of two
-    per = 40.0 * (bits - 2) + 88.0 * (bits - 1) + 48.0
-    return float(per.mean())
+    ref = 40.0 * (bits - 3) + 128.0 * (bits - 1)
+    run = 40.0 * (bits - 2) + 80.0 * (bits - 1) + 48.0
+    return float(ref.mean()), float(run.mean())
 
 
 class ClockSampler:
@@ -160,6 +170,10 @@ def run_reference(args):
         return 0
     threads = os.cpu_count() or 1
     sample_n = args.cpu_sample
+    if sample_n <= 0:  # each step about --cpu-seconds / 8 of CPU time
+        probe, _ = Oracle().random_primes(SEED, 1 << 18, threads)
+        r0, _, _ = cpu_reference_rate(probe, threads)
+        sample_n = max(1 << 20, int(r0 * args.cpu_seconds / 8))
     primes, _ = Oracle().random_primes(SEED, sample_n, threads)
     rates, times = [], []
     for i in range(args.warmup + args.steps):
@@ -181,14 +195,69 @@ def run_reference(args):
     return 0
 
 
-def run_batched_vs_plain(ww, local: int, n_units: int, tune_units: int = 32):
-    """Config 4 subsample: the first n_units of the seed-11 uneven mix (widths
-    log-uniform in [1e6, 1e10], starts uniform in [1e15, 2^64-1e10], multiples
-    of 30).  Plain = one range per launch sequence (clear, sieve, test, read)
+def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30) -> dict:
+    """The plain one-range path over [2^64-2^35, 2^64-2^35+width): per 2^30
+    numbers (the checkpoint cadence) clear, sieve + SPRP, both tests, sync and
+    read the counters back, as the reference program's loop does.  With the
+    default width 2^34 this is the whole range of tests/golden/ref_long.json,
+    whose reference checksum the result is compared with."""
+    lo = 2**64 - 2**35
+    hi = lo + width
+    ctx = ww.Context(local, max_prps=ww.prp_count_bound(0, ckpt), max_hits=15000)
+    ctx.run_range(lo, min(hi, lo + ckpt))  # warm
+
+    # sieve and test kernel times of one full checkpoint segment
+    ctx.clear_results()
+    ctx.clear_segment()
+    ctx.marker(0)
+    ctx.sieve_prp(lo, min(hi, lo + ckpt))
+    ctx.marker(1)
+    ctx.test_prps()
+    ctx.marker(2)
+    ctx.sync()
+    seg_prps = ctx.counters()["total_prp_count"]
+    sieve_ms, test_ms = ctx.elapsed_ms(0, 1), ctx.elapsed_ms(1, 2)
+
+    cks, cnt, res = 0, 0, 0
+    ctx.marker(3)
+    t0 = time.perf_counter()
+    start = lo
+    while start < hi:
+        stop = min(start + ckpt, hi)
+        ctx.clear_results()
+        ctx.clear_segment()
+        ctx.sieve_prp(start, stop)
+        ctx.test_prps()
+        k = ctx.counters()  # sync + read-back at every checkpoint
+        if k["overflow"]:
+            raise SystemExit(f"range leg overflow flag {k['overflow']}")
+        cks, cnt, res = (cks + k["checksum"]) % 2**64, cnt + k["total_prp_count"], res + k["result_count"]
+        start = stop
+    wall = time.perf_counter() - t0
+    ctx.marker(4)
+    ctx.sync()
+    dev_ms = ctx.elapsed_ms(3, 4)
+    ctx.close()
+    out = {"workload": f"plain path over [2^64-2^35, 2^64-2^35+{width}), checkpoint every 2^30 numbers",
+           "numbers": width, "prps": cnt, "device_ms": dev_ms, "wall_s": wall,
+           "primes_per_s": cnt / wall, "numbers_per_s": width / wall,
+           "segment_2p30": {"prps": seg_prps, "sieve_ms": sieve_ms, "test_ms": test_ms,
+                            "sieve_numbers_per_s": min(width, ckpt) / (sieve_ms * 1e-3),
+                            "test_primes_per_s": seg_prps / (test_ms * 1e-3)},
+           "checksum": "%016X" % cks, "results": res}
+    golden = ROOT / "tests" / "golden" / "ref_long.json"
+    if golden.exists():
+        g = json.loads(golden.read_text())["config3"]
+        if g["lo"] == lo and g["hi"] == hi:
+            out["reference_checksum_equal"] = bool(out["checksum"] == g["checksum"] and cnt == g["prp_count"])
+    return out
+
+
+def compare_batched_plain(ww, local: int, units: list, workload: str, tune_units: int = 32) -> dict:
+    """Plain = one range per launch sequence (clear, sieve, test, read)
     through the context API; batched = one persistent CUDA-graph launch over
     the tile queue after the autotuner picked the configuration.  Per-unit
     checksums and PRP counts must agree."""
-    units = ww.uneven_units(11, 4096)[:n_units]
     ctx = ww.Context(local, max_prps=ww.prp_count_bound(0, 1 << 30), max_hits=15000)
     b = ww.Batch(ctx)
     cfg, _ = b.tune(units[:tune_units])
@@ -199,9 +268,9 @@ def run_batched_vs_plain(ww, local: int, n_units: int, tune_units: int = 32):
     ctx.sync()
     batch_ms = ctx.elapsed_ms(0, 1)
     prps = sum(r["prp_count"] for r in res)
-    # plain, config 3's definition: per range, sieve -> Wieferich -> WSS kernels
-    # with a checkpoint (sync, counters and hits read back, clear) every 2^30
-    # numbers and at the range's end
+    # plain, the reference program's flow: per range, sieve -> Wieferich ->
+    # WSS kernels with a checkpoint (sync, counters and hits read back,
+    # clear) every 2^30 numbers and at the range's end
     ckpt = 1 << 30
     t0 = time.perf_counter()
     plain = []
@@ -233,17 +302,31 @@ def run_batched_vs_plain(ww, local: int, n_units: int, tune_units: int = 32):
                 for r, a, p in zip(res, alone, plain))
     ctx.close()
     numbers = sum(z - a for a, z in units)
-    return {"workload": f"first {n_units} units of the seed-11 uneven mix (config 4)", "units": n_units,
+    return {"workload": workload, "units": len(units),
             "numbers": numbers, "prps": prps, "batched_primes_per_s": prps / (batch_ms * 1e-3),
             "plain_primes_per_s": prps / plain_s, "plain_fused_primes_per_s": prps / fused_s,
             "batched_numbers_per_s": numbers / (batch_ms * 1e-3),
             "speedup_batched_vs_plain": plain_s / (batch_ms * 1e-3),
             "speedup_batched_vs_plain_fused": fused_s / (batch_ms * 1e-3),
             "plain_definition": "per range: sieve, Wieferich, WSS kernels; checkpoint sync + read-back "
-                                "every 2^30 numbers (config 3)",
+                                "every 2^30 numbers (the reference program's loop)",
             "per_unit_bit_identical": bool(equal),
             "tuned_config": {"seg_words": cfg[0], "seg_bytes": 4 * cfg[0], "threads": cfg[1],
                              "primes_per_thread": cfg[2]}}
+
+
+def run_batched_vs_plain(ww, local: int, n_units: int) -> dict:
+    """The seed-11 uneven mix (4096 units, widths log-uniform in [1e6, 1e10],
+    starts uniform in [1e15, 2^64-1e10], multiples of 30): its first n_units
+    units, and separately its first 2*n_units units narrower than 1e8 (where
+    one launch sequence per range leaves most of the GPU idle)."""
+    mix = ww.uneven_units(11, 4096)
+    out = compare_batched_plain(ww, local, mix[:n_units],
+                                f"first {n_units} units of the seed-11 uneven mix (4096 units)")
+    narrow = [u for u in mix if u[1] - u[0] < 10**8][: 2 * n_units]
+    out["narrow_units"] = compare_batched_plain(
+        ww, local, narrow, f"first {len(narrow)} units of the same mix narrower than 1e8")
+    return out
 
 
 def run_serving(ww, local: int, seconds: float, rate: float = 200.0, seed: int = 13, check_cpu: int = 12):
@@ -336,8 +419,11 @@ def main():
     ctx.load_prps_ptr(host_ptr, n)
     ctx.sync()
 
-    # IMAD pipe peak on this device, at this moment (roofline denominator)
-    imad_peak, _ = ww.pipe_bench(0, device=local)
+    # integer-multiply peaks on this device, at this moment (roofline
+    # denominators): the 64x64->128 mad.lo/mad.hi carry chain the op count is
+    # made of (8 multiply instructions per product), and mad.lo alone
+    chain_peak, _ = ww.pipe_bench(3, device=local)
+    madlo_peak, _ = ww.pipe_bench(0, device=local)
 
     def step():
         ctx.clear_results()
@@ -376,8 +462,8 @@ def main():
     barrier()
     t_e0 = time.perf_counter()
     for _ in range(args.steps):
-        ctx.load_prps_ptr(host_ptr, n)
-        step()
+        ctx.clear_results()
+        ctx.test_prps_host_ptr(host_ptr, n)  # H2D copy of each chunk overlaps the test of the previous one
         k = ctx.counters()
         if k["result_count"]:
             ctx.hits()
@@ -388,6 +474,7 @@ def main():
         torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
     e2e_value = n * world * args.steps / float(te.item())
     hits_per_step = k["result_count"]
+    e2e_checksum = k["checksum"]
 
     if world > 1:
         torch.distributed.barrier()
@@ -398,13 +485,21 @@ def main():
         return 0
 
     # ---- roofline (IMAD pipe) and CPU baseline on rank 0
-    per_prime = algorithmic_imad_per_prime(primes)
+    per_prime, per_prime_run = algorithmic_imad_per_prime(primes)
     launch_ms = dev_ms / args.steps
     achieved = per_prime * n / (launch_ms * 1e-3)
-    roofline = {"bound": "imad", "achieved": achieved / 1e12, "peak": imad_peak / 1e12, "unit": "Tops/s",
-                "frac": achieved / imad_peak, "traffic": profile_traffic(),
-                "peak_source": "measured live: mad.lo.u32 chains on every SM (ww_pipe_bench mode 0)",
+    achieved_run = per_prime_run * n / (launch_ms * 1e-3)
+    roofline = {"bound": "imad", "achieved": achieved / 1e12, "peak": chain_peak / 1e12, "unit": "Tops/s",
+                "frac": achieved / chain_peak, "traffic": profile_traffic(),
+                "peak_source": "measured live: 64x64->128 mad.lo.cc/madc.hi carry chains on every SM, per "
+                               "multiply instruction (ww_pipe_bench mode 3)",
                 "ops_per_prime": per_prime,
+                "ops_source": "reference kernels' algorithm: 40(k-3) + 128(k-1) 32-bit multiplies per prime",
+                "executed": {"ops_per_prime": per_prime_run, "achieved": achieved_run / 1e12,
+                             "frac": achieved_run / chain_peak,
+                             "note": "multiplies k_test_prps itself runs: 40(k-2) + 80(k-1) + 48"},
+                "mad_lo_only": {"peak": madlo_peak / 1e12, "frac": achieved / madlo_peak,
+                                "frac_executed": achieved_run / madlo_peak},
                 "hbm": {"bytes_per_launch": 16 * n, "GBps": 16 * n / (launch_ms * 1e-3) / 1e9,
                         "peak_GBps": json.loads(PEAKS.read_text())["hbm_gbs"] if PEAKS.exists() else 6650.0}}
 
@@ -412,7 +507,11 @@ def main():
     if not args.no_cpu_baseline:
         try:
             threads = os.cpu_count() or 1
-            sample = primes[: min(args.cpu_sample, n)]
+            take = args.cpu_sample
+            if take <= 0:  # calibrate on 2^18 primes, then size the sample to --cpu-seconds
+                r0, _, _ = cpu_reference_rate(primes[: 1 << 18], threads)
+                take = max(1 << 20, int(r0 * args.cpu_seconds))
+            sample = primes[: min(take, n)]
             rate, cks_cpu, dt = cpu_reference_rate(sample, threads)
             ctx2 = ww.Context(local, max_prps=sample.size, max_hits=15000)
             ctx2.load_prps(sample)
@@ -428,6 +527,8 @@ def main():
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 
     extra = {}
+    if args.range_width:
+        extra["range_pipeline"] = run_range_pipeline(ww, local, int(args.range_width))
     if args.batch_units:
         extra["batched_vs_plain"] = run_batched_vs_plain(ww, local, args.batch_units)
     if args.serve_seconds:
@@ -438,7 +539,9 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": config(args, world), **extra,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
-                    "d2h_bytes_per_step": 32 + hit_bytes * hits_per_step},
+                    "d2h_bytes_per_step": 32 + hit_bytes * hits_per_step,
+                    "call": "ww_test_prps_host (pinned list, copy of chunk k+1 overlapping the test of chunk k) "
+                            "+ ww_read_counters", "checksum_equal": bool(e2e_checksum == checksum)},
             "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu,
             "clocks": clocks.summary(), "checksum": "%016X" % checksum, "list_gen_s": gen_s}
     print(json.dumps(line))

@@ -155,6 +155,15 @@ int ww_test_prps(ww_ctx *ctx); /* fused wieferich + wallsunsun */
  * count, q computed on the device).  For fixed-list workloads. */
 int ww_load_prps(ww_ctx *ctx, const uint64_t *host_primes, uint64_t n);
 
+/* Both tests over a host list of PRPs, accumulating into the context's
+ * checksum, PRP count and hit list like ww_load_prps + ww_test_prps.  The
+ * list moves in chunks through the two halves of the PRP buffer on a second
+ * stream, so the copy of one chunk overlaps the test of the previous one
+ * (pinned host memory is needed for the overlap).  Returns when the work is
+ * queued; read the counters after ww_sync.  No counterpart in the reference,
+ * whose lists come from getsegprimes on the device. */
+int ww_test_prps_host(ww_ctx *ctx, const uint64_t *host_primes, uint64_t n);
+
 /* Record an event after the work queued so far; ww_wait_marker blocks until
  * the event `slot` (0..7) completed or timeout_ms passed (the reference's
  * launchEvent / waitOnEvent, main.cpp:329-377). */
@@ -270,7 +279,8 @@ typedef struct {
 typedef struct {
     uint64_t prp_pool_bytes; /* device memory for per-request PRP buffers */
     uint32_t max_active;     /* device slots */
-    uint32_t epoch_tiles;    /* most tiles one step launches */
+    uint32_t epoch_tiles;    /* tiles one step launches (rounded to whole
+                                waves of resident CTAs when above one wave) */
     uint32_t max_hits;       /* hit records per step */
     uint32_t store_prps;     /* 1: keep each request's PRP list on the device */
 } ww_server_cfg;

@@ -113,6 +113,30 @@ def test_hits_match_oracle(ctx, oracle):
     assert sorted(got["hits"]) == sorted(want)
 
 
+def test_host_list_pipeline_matches_loaded_list(ww, oracle, ref_terms):
+    """ww_test_prps_host (chunked copy/test overlap) against ww_load_prps +
+    ww_test_prps and the oracle: checksum, count and hits, over a list that
+    spans several chunks of both buffer halves, including the known hits."""
+    ps, _ = ww.random_primes(11, 3 * (1 << 20) + 12345)
+    ps = np.concatenate([ps, ref_terms["known_hits_p"], ref_terms["small_p"]])
+    with ww.Context(0, max_prps=1 << 21, max_hits=15000) as c:
+        c.clear_results()
+        c.test_prps_host(ps)
+        got = c.counters()
+        got_hits = sorted(c.hits())
+    with ww.Context(0, max_prps=ps.size, max_hits=15000) as c:
+        c.load_prps(ps)
+        c.clear_results()
+        c.test_prps()
+        c.sync()
+        want = c.counters()
+        want_hits = sorted(c.hits())
+    assert got["checksum"] == want["checksum"] and got["total_prp_count"] == ps.size == want["total_prp_count"]
+    assert got["result_count"] == want["result_count"] > 0 and got_hits == want_hits
+    summ, ohits = oracle.test_list(ps, hit_cap=15000)
+    assert summ["checksum"] == got["checksum"] and sorted(ohits) == got_hits
+
+
 def test_prp_overflow_is_reported(ww, oracle):
     with ww.Context(0, max_prps=1000, max_hits=100) as c:
         c.clear_results()

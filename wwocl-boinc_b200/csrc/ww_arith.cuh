@@ -17,6 +17,14 @@
 
 #include <stdint.h>
 
+// On the device the modular corrections (REDC's final subtraction, the
+// two-digit subtraction, the finish of a two-digit product) are written as
+// PTX borrow chains with a mask instead of compare + select; measured 1-2 %
+// faster on the fused test kernel.  -DWW_NO_PTX_CC selects the C forms.
+#if !defined(WW_NO_PTX_CC) && !defined(WW_PTX_CC)
+#define WW_PTX_CC 1
+#endif
+
 #if defined(__CUDACC__)
 #define WW_HD __host__ __device__ __forceinline__
 #else
@@ -73,7 +81,18 @@ WW_HD u64 sub_mod(u64 a, u64 b, u64 n) {  // a < n, b <= n
 WW_HD u64 redc(u64 lo, u64 hi, u64 n, u64 q) {
     u64 u = lo * q;
     u64 v = mul_hi(u, n);
+#if defined(__CUDA_ARCH__) && defined(WW_PTX_CC)
+    u64 r;
+    asm("{\n\t.reg .u64 m;\n\t"
+        "sub.cc.u64 %0, %1, %2;\n\t"  // hi - v, borrow-out
+        "subc.u64 m, 0, 0;\n\t"       // -borrow
+        "and.b64 m, m, %3;\n\t"
+        "add.u64 %0, %0, m;\n\t}"
+        : "=&l"(r) : "l"(hi), "l"(v), "l"(n));
+    return r;
+#else
     return hi >= v ? hi - v : hi - v + n;
+#endif
 }
 
 WW_HD u64 mont_mul(u64 a, u64 b, u64 n, u64 q) {
@@ -139,11 +158,28 @@ WW_HD D2 m2_add(D2 x, D2 y, u64 p) {
 
 WW_HD D2 m2_sub(D2 x, D2 y, u64 p) {
     D2 r;
+#if defined(__CUDA_ARCH__) && defined(WW_PTX_CC)
+    // one borrow chain through both digits; each digit adds p back on its
+    // own borrow-out
+    asm("{\n\t.reg .u64 m0, m1;\n\t"
+        "sub.cc.u64 %0, %2, %4;\n\t"
+        "subc.u64 m0, 0, 0;\n\t"       // reads the low borrow, keeps it
+        "subc.cc.u64 %1, %3, %5;\n\t"  // x1 - y1 - borrow
+        "subc.u64 m1, 0, 0;\n\t"
+        "and.b64 m0, m0, %6;\n\t"
+        "and.b64 m1, m1, %6;\n\t"
+        "add.u64 %0, %0, m0;\n\t"
+        "add.u64 %1, %1, m1;\n\t}"
+        : "=&l"(r.d0), "=&l"(r.d1)
+        : "l"(x.d0), "l"(x.d1), "l"(y.d0), "l"(y.d1), "l"(p));
+    return r;
+#else
     bool b = x.d0 < y.d0;
     r.d0 = b ? x.d0 - y.d0 + p : x.d0 - y.d0;
     u64 t = y.d1 + (u64)b;  // <= p
     r.d1 = x.d1 >= t ? x.d1 - t : x.d1 - t + p;
     return r;
+#endif
 }
 
 WW_HD D2 m2_dbl(D2 x, u64 p) { return m2_add(x, x, p); }
@@ -155,6 +191,39 @@ WW_HD D2 m2_finish(u64 alo, u64 ahi, u64 clo, u64 chi, u64 ctop, u64 p, u64 q) {
     const u64 u = alo * q;
     const u64 v = mul_hi(u, p);
     D2 r;
+#if defined(__CUDA_ARCH__) && defined(WW_PTX_CC)
+    u64 mb, s, h, k, h2;
+    // low digit ahi - v, plus p on borrow; mb = -borrow
+    asm("{\n\t.reg .u64 t;\n\t"
+        "sub.cc.u64 %0, %2, %3;\n\t"
+        "subc.u64 %1, 0, 0;\n\t"
+        "and.b64 t, %1, %4;\n\t"
+        "add.u64 %0, %0, t;\n\t}"
+        : "=&l"(r.d0), "=&l"(mb) : "l"(ahi), "l"(v), "l"(p));
+    // (k:h) = (C + u) >> 64 < 2p, s = low word of C + u
+    asm("add.cc.u64 %0, %3, %4;\n\t"
+        "addc.cc.u64 %1, %5, 0;\n\t"
+        "addc.u64 %2, %6, 0;"
+        : "=&l"(s), "=&l"(h), "=&l"(k) : "l"(clo), "l"(u), "l"(chi), "l"(ctop));
+    // h2 = (k:h) mod p: subtract p; the high word k - borrow is -1 exactly
+    // when (k:h) < p, and then p is added back
+    asm("{\n\t.reg .u64 m;\n\t"
+        "sub.cc.u64 %0, %1, %2;\n\t"
+        "subc.u64 m, %3, 0;\n\t"
+        "shr.s64 m, m, 1;\n\t"
+        "and.b64 m, m, %2;\n\t"
+        "add.u64 %0, %0, m;\n\t}"
+        : "=&l"(h2) : "l"(h), "l"(p), "l"(k));
+    const u64 v2 = mul_hi(s * q, p);
+    const u64 t = v2 - mb;  // v2 + borrow <= p
+    asm("{\n\t.reg .u64 m;\n\t"
+        "sub.cc.u64 %0, %1, %2;\n\t"
+        "subc.u64 m, 0, 0;\n\t"
+        "and.b64 m, m, %3;\n\t"
+        "add.u64 %0, %0, m;\n\t}"
+        : "=&l"(r.d1) : "l"(h2), "l"(t), "l"(p));
+    return r;
+#else
     const bool b = ahi < v;
     r.d0 = b ? ahi - v + p : ahi - v;
     // C + u
@@ -169,6 +238,7 @@ WW_HD D2 m2_finish(u64 alo, u64 ahi, u64 clo, u64 chi, u64 ctop, u64 p, u64 q) {
     const u64 t = v2 + (u64)b;  // <= p
     r.d1 = h >= t ? h - t : h - t + p;
     return r;
+#endif
 }
 
 WW_HD D2 m2_mul(D2 x, D2 y, u64 p, u64 q) {

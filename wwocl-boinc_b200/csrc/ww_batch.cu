@@ -662,7 +662,10 @@ int ww_server_step(ww_ctx *ctx, ww_request_result *done, uint32_t cap, uint32_t 
     a.n_units = n;
     a.rr = s.d_rr;
     a.epoch_tiles = s.d_epoch;
-    a.budget = s.cfg.epoch_tiles;
+    // whole waves of the resident CTAs: a partial last wave would leave most
+    // SMs idle while its few tiles finish
+    const u32 g = (u32)s.grid;
+    a.budget = s.cfg.epoch_tiles < g ? s.cfg.epoch_tiles : std::max(1u, (s.cfg.epoch_tiles + g / 2) / g) * g;
     a.hit_p = s.d_hit_p;
     a.hit_result = s.d_hit_res;
     a.hit_rem = s.d_hit_rem;
@@ -671,7 +674,7 @@ int ww_server_step(ww_ctx *ctx, ww_request_result *done, uint32_t cap, uint32_t 
     a.hit_count = s.d_hit_count;
     a.hit_capacity = s.cfg.max_hits;
     a.overflow = s.d_overflow;
-    const int grid = std::min<int>(s.grid, (int)s.cfg.epoch_tiles);
+    const int grid = std::min<int>(s.grid, (int)a.budget);
     s.e->serve_kernel<<<grid, s.e->threads, s.e->smem, st>>>(a);
     WW_CU(cudaGetLastError());
     WW_CU(cudaMemcpyAsync(s.h_slots, s.d_slots, (size_t)n * sizeof(UnitState), cudaMemcpyDeviceToHost, st));

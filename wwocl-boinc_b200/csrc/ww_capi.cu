@@ -64,7 +64,31 @@ int wheel_index_of(uint64_t n) {
     }
 }
 
-int test_grid() { return sm_count() * 4; }
+// One full wave of resident CTAs: the test kernels split the list evenly
+// over the grid (grid-stride loop), so a grid above the resident count would
+// leave its last CTAs running as a thinly occupied second wave.
+template <class Kernel>
+int resident_grid(Kernel k, int threads) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, 0) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    return sm_count() * per_sm;
+}
+
+int test_grid() {
+    static const int g = resident_grid(k_test_prps, kTestThreads);
+    return g;
+}
+int wieferich_grid() {
+    static const int g = resident_grid(k_wieferich, kTestThreads);
+    return g;
+}
+int wallsunsun_grid() {
+    static const int g = resident_grid(k_wallsunsun, kTestThreads);
+    return g;
+}
 
 }  // namespace
 
@@ -146,7 +170,7 @@ int ww_launch_wieferich(uint32_t *primecount, const uint64_t *g_prime, const uin
         !resultcount || !totalprimecount || !overflow)
         return set_err("null pointer"), WW_ERR_ARG;
     HitOut h{(u64 *)special_prime, rem, quot, result, resultcount, numresults, overflow};
-    k_wieferich<<<test_grid(), kTestThreads, 0, as_stream(stream)>>>(
+    k_wieferich<<<wieferich_grid(), kTestThreads, 0, as_stream(stream)>>>(
         primecount, (const u64 *)g_prime, (const u64 *)g_invert, (u64 *)g_one, h, (u64 *)checksum,
         (u64 *)totalprimecount, capacity);
     WW_CHECK_LAUNCH();
@@ -162,7 +186,7 @@ int ww_launch_wallsunsun(const uint32_t *primecount, const uint64_t *g_prime,
         !resultcount || !overflow)
         return set_err("null pointer"), WW_ERR_ARG;
     HitOut h{(u64 *)special_prime, rem, quot, result, resultcount, numresults, overflow};
-    k_wallsunsun<<<test_grid(), kTestThreads, 0, as_stream(stream)>>>(
+    k_wallsunsun<<<wallsunsun_grid(), kTestThreads, 0, as_stream(stream)>>>(
         primecount, (const u64 *)g_prime, (const u64 *)g_invert, (const u64 *)g_one, h,
         (u64 *)checksum, capacity);
     WW_CHECK_LAUNCH();
@@ -233,7 +257,15 @@ struct ww_ctx {
     int *hrem = nullptr, *hquot = nullptr, *hres = nullptr;
     u32 hcap = 0;
     cudaEvent_t ev[8] = {};
+    // ww_test_prps_host: copy stream, per-half events, per-chunk counts
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copied[2] = {}, consumed[2] = {};
+    u32 *d_chunk = nullptr, *h_chunk = nullptr;  // [2 * kHostChunksMax]: count, max
 };
+
+namespace {
+constexpr u64 kHostChunksMax = 1024;
+}
 
 extern "C" {
 
@@ -276,6 +308,14 @@ void ww_close(ww_ctx *c) {
     cudaFree(c->hres);
     cudaFree(c->dc);
     if (c->hc) cudaFreeHost(c->hc);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    cudaFree(c->d_chunk);
+    if (c->h_chunk) cudaFreeHost(c->h_chunk);
+    for (int i = 0; i < 2; ++i) {
+        if (c->copied[i]) cudaEventDestroy(c->copied[i]);
+        if (c->consumed[i]) cudaEventDestroy(c->consumed[i]);
+    }
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     for (int i = 0; i < 8; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -408,6 +448,58 @@ int ww_load_prps(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
         if (blocks > (uint64_t)sm_count() * 8) blocks = (uint64_t)sm_count() * 8;
         k_fill_inverse<<<(unsigned)blocks, 256, 0, c->stream>>>(c->prime, c->inv, n);
         WW_CHECK_LAUNCH();
+    }
+    return WW_OK;
+}
+
+int ww_test_prps_host(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
+    WW_NEED_BUFFERS(c);
+    if (!host_primes && n) return set_err("null list"), WW_ERR_ARG;
+    if (n == 0) return WW_OK;
+    if (c->cap < 2) return set_err("PRP buffer too small for double buffering"), WW_ERR_ARG;
+    WW_CU(cudaSetDevice(c->device));
+    if (!c->copy_stream) {
+        WW_CU(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; ++i) {
+            WW_CU(cudaEventCreateWithFlags(&c->copied[i], cudaEventDisableTiming));
+            WW_CU(cudaEventCreateWithFlags(&c->consumed[i], cudaEventDisableTiming));
+        }
+        WW_CU(cudaMalloc(&c->d_chunk, 2 * kHostChunksMax * sizeof(u32)));
+        WW_CU(cudaMallocHost(&c->h_chunk, 2 * kHostChunksMax * sizeof(u32)));
+    }
+    // chunk: about an eighth of the list (at least 2^20 PRPs), at most half
+    // the buffer, and few enough chunks for the count table
+    u64 chunk = std::max<u64>(1ull << 20, (n + 7) / 8);
+    chunk = std::max<u64>(chunk, (n + kHostChunksMax - 1) / kHostChunksMax);
+    chunk = std::min<u64>(chunk, std::min<u64>(c->cap / 2, 0xffffffffull));
+    const u64 nchunks = (n + chunk - 1) / chunk;
+    if (nchunks > kHostChunksMax)
+        return set_err("list of %llu PRPs needs a PRP buffer of at least %llu entries", (unsigned long long)n,
+                       (unsigned long long)(2 * ((n + kHostChunksMax - 1) / kHostChunksMax))), WW_ERR_ARG;
+    // the previous call's kernels may still read the count table
+    WW_CU(cudaStreamSynchronize(c->stream));
+    for (u64 i = 0; i < nchunks; ++i) {
+        c->h_chunk[2 * i] = (u32)std::min<u64>(chunk, n - i * chunk);
+        c->h_chunk[2 * i + 1] = 0;
+    }
+    WW_CU(cudaMemcpyAsync(c->d_chunk, c->h_chunk, 2 * nchunks * sizeof(u32), cudaMemcpyHostToDevice, c->stream));
+    // the copy stream must not overwrite a half that earlier test work still reads
+    WW_CU(cudaEventRecord(c->consumed[0], c->stream));
+    WW_CU(cudaEventRecord(c->consumed[1], c->stream));
+    HitOut h{c->hprime, c->hrem, c->hquot, c->hres, &c->dc->resultcount, c->hcap, &c->dc->overflow};
+    for (u64 i = 0; i < nchunks; ++i) {
+        const int half = (int)(i & 1);
+        u64 *dst = c->prime + (u64)half * chunk;
+        const u64 len = c->h_chunk[2 * i];
+        WW_CU(cudaStreamWaitEvent(c->copy_stream, c->consumed[half], 0));
+        WW_CU(cudaMemcpyAsync(dst, host_primes + i * chunk, len * 8, cudaMemcpyHostToDevice, c->copy_stream));
+        WW_CU(cudaEventRecord(c->copied[half], c->copy_stream));
+        WW_CU(cudaStreamWaitEvent(c->stream, c->copied[half], 0));
+        k_test_prps<<<test_grid(), kTestThreads, 0, c->stream>>>(c->d_chunk + 2 * i, dst, nullptr, h,
+                                                                 (u64 *)&c->dc->checksum, (u64 *)&c->dc->total,
+                                                                 len);
+        WW_CHECK_LAUNCH();
+        WW_CU(cudaEventRecord(c->consumed[half], c->stream));
     }
     return WW_OK;
 }

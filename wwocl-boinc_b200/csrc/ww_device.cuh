@@ -17,7 +17,10 @@ constexpr int kSieveThreads = 256;
 constexpr int kSieveWarps = kSieveThreads / 32;
 constexpr int kWordsPerThread = kSegWords / kSieveThreads;
 constexpr int kQueueCap = 640;  // 31 carried + 32 words x at most 18 survivors
-constexpr int kTestThreads = 256;
+#ifndef WW_TEST_THREADS
+#define WW_TEST_THREADS 256
+#endif
+constexpr int kTestThreads = WW_TEST_THREADS;
 #ifndef WW_TEST_MINB
 #define WW_TEST_MINB 1  // minimum resident CTAs per SM asked of the test kernels
 #endif
@@ -118,9 +121,20 @@ __device__ __forceinline__ void deep_unmark(u32 *bitmap, const u32 *rescue, u32 
     }
 }
 
-// Mark every odd multiple of the deep primes in the segment.
+// Mark every odd multiple of the deep primes in the segment.  The smallest
+// primes have the most multiples: each of the first kDeepWarpPrimes primes
+// is marked by a whole warp (lane l takes every 32nd multiple), the rest one
+// prime per thread, so no thread holds the others at the next barrier.
+constexpr int kDeepWarpPrimes = 512;
+
 __device__ __forceinline__ void deep_mark(u64 first, u32 nvalid, u32 *bitmap, int tid, int nthreads) {
-    for (int i = tid; i < WW_DEEP_COUNT; i += nthreads) {
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nthreads >> 5;
+    for (int i = warp; i < kDeepWarpPrimes; i += nwarps) {
+        const uint4 e = kDeepDev[i];
+        const u32 j0 = deep_first_multiple(first, e.x, e.z);
+        for (u32 j = j0 + (u32)lane * e.x; j < nvalid; j += 32u * e.x) atomicOr(&bitmap[j >> 5], 1u << (j & 31));
+    }
+    for (int i = kDeepWarpPrimes + tid; i < WW_DEEP_COUNT; i += nthreads) {
         const uint4 e = kDeepDev[i];
         for (u32 j = deep_first_multiple(first, e.x, e.z); j < nvalid; j += e.x)
             atomicOr(&bitmap[j >> 5], 1u << (j & 31));

@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "boinc_shim.hpp"
 #include "wwcuda.h"
 
 namespace wwhost {
@@ -38,7 +39,8 @@ struct State {
 inline void write_state(const Files &f, uint64_t start, uint64_t stop, const State &s, bool &write_a_next) {
     ww_state st{s.current, s.cksm, s.psum, s.pcnt, 0};
     int a = write_a_next ? 1 : 0;
-    if (ww_state_write(f.state_a.c_str(), f.state_b.c_str(), start, stop, &st, &a) != WW_OK)
+    const std::string fa = boinc::resolve_filename(f.state_a), fb = boinc::resolve_filename(f.state_b);
+    if (ww_state_write(fa.c_str(), fb.c_str(), start, stop, &st, &a) != WW_OK)
         fprintf(stderr, "Cannot write state !!! Continuing... (%s)\n", ww_last_error());
     write_a_next = a != 0;
 }
@@ -46,7 +48,8 @@ inline void write_state(const Files &f, uint64_t start, uint64_t stop, const Sta
 inline bool read_state(const Files &f, uint64_t start, uint64_t stop, State &s, bool &write_a_next) {
     ww_state st{};
     int a = 1;
-    if (ww_state_read(f.state_a.c_str(), f.state_b.c_str(), start, stop, &st, &a) != 1) return false;
+    const std::string fa = boinc::resolve_filename(f.state_a), fb = boinc::resolve_filename(f.state_b);
+    if (ww_state_read(fa.c_str(), fb.c_str(), start, stop, &st, &a) != 1) return false;
     s.current = st.current;
     s.cksm = st.cksm;
     s.psum = st.psum;
@@ -58,7 +61,7 @@ inline bool read_state(const Files &f, uint64_t start, uint64_t stop, State &s, 
 // report_solution (main.cpp:741-765): append and fsync.  Returns false on
 // failure (the caller exits, as the reference does).
 inline bool report_solution(const Files &f, const std::string &text) {
-    FILE *r = fopen(f.results.c_str(), "a");
+    FILE *r = boinc::fopen_resolved(f.results, "a");
     if (!r) {
         fprintf(stderr, "Cannot open %s !!!\n", f.results.c_str());
         return false;
@@ -75,7 +78,7 @@ inline bool report_solution(const Files &f, const std::string &text) {
 }
 
 inline bool truncate_results(const Files &f) {
-    FILE *r = fopen(f.results.c_str(), "w");  // main.cpp:1535-1540
+    FILE *r = boinc::fopen_resolved(f.results, "w");  // main.cpp:1535-1540
     if (!r) return false;
     fclose(r);
     return true;

@@ -321,7 +321,7 @@ int main(int argc, char **argv) {
         printf("Workunit complete.\n");
         fprintf(stderr, "Workunit complete.\n");
         ww_close(ctx);
-        return 0;
+        boinc::finish(0);
     }
 
     const double target_ms = o.compute ? 100.0 : (o.ws ? (double)o.ws : 10.0);
@@ -354,7 +354,9 @@ int main(int argc, char **argv) {
         }
         const double t = now_s();
         if (t - last_progress > 1.0) {  // main.cpp:1699-1708
-            printf("Tests done: %.4f%%\n", (double)(start - bottom) / (double)(top - bottom) * 100.0);
+            const double fd = (double)(start - bottom) / (double)(top - bottom);
+            boinc::fraction_done(fd);
+            if (boinc::is_standalone()) printf("Tests done: %.4f%%\n", fd * 100.0);
             last_progress = t;
         }
         enqueue_segment(ctx, start, stop, o.separate);
@@ -371,6 +373,7 @@ int main(int argc, char **argv) {
         if (ckpt_secs > 60.0 || stop == top || by_count) {  // main.cpp:1743-1792
             must(ww_sync(ctx, 0), "sync");
             iter = 0;
+            boinc::begin_critical_section();
             get_results(ctx, o, now_s() - last_ckpt, st, mem_size);
             if (stop == top) {
                 char buffer[64];
@@ -380,15 +383,18 @@ int main(int argc, char **argv) {
                 printf("Workunit complete. Average speed: %.2f Million primes per second.\n", p_avg);
                 fprintf(stderr, "Workunit complete. Average speed: %.2f Million primes per second.\n", p_avg);
                 printf("Checksum: %016" PRIX64 "\n", st.cksm);
+                boinc::fraction_done(1.0);
             }
             st.current = stop;
-            write_state(o.files, bottom, top, st, write_a_next);
-            printf("Checkpoint, current: %" PRIu64 "\n", stop);
+            write_state(o.files, bottom, top, st, write_a_next);  // checkpoint(), main.cpp:212-221
+            if (boinc::is_standalone()) printf("Checkpoint, current: %" PRIu64 "\n", stop);
+            boinc::checkpoint_completed();
+            boinc::end_critical_section();
             last_ckpt = now_s();
             since_ckpt = 0;
             must(ww_clear_results(ctx), "clearresult");
         }
     }
     ww_close(ctx);
-    return 0;
+    boinc::finish(0);
 }

@@ -113,6 +113,7 @@ _SIGS = {
     "ww_wallsunsun": (C.c_int, [_VP]),
     "ww_test_prps": (C.c_int, [_VP]),
     "ww_load_prps": (C.c_int, [_VP, _VP, C.c_uint64]),
+    "ww_test_prps_host": (C.c_int, [_VP, _VP, C.c_uint64]),
     "ww_marker": (C.c_int, [_VP, C.c_int]),
     "ww_wait_marker": (C.c_int, [_VP, C.c_int, C.c_uint32]),
     "ww_marker_elapsed": (C.c_int, [_VP, C.c_int, C.c_int, C.POINTER(C.c_float)]),
@@ -336,6 +337,16 @@ class Context:
 
     def load_prps_ptr(self, host_ptr: int, n: int) -> None:
         check(_L.ww_load_prps(self.h, host_ptr, n), "ww_load_prps")
+
+    def test_prps_host(self, primes: np.ndarray) -> None:
+        """Both tests over a host list, copy and test pipelined in chunks."""
+        primes = np.ascontiguousarray(primes, dtype=np.uint64)
+        check(_L.ww_test_prps_host(self.h, primes.ctypes.data, primes.size), "ww_test_prps_host")
+        self.sync()  # the pageable source must outlive the copies
+
+    def test_prps_host_ptr(self, host_ptr: int, n: int) -> None:
+        """As test_prps_host for a pinned host buffer; returns once queued."""
+        check(_L.ww_test_prps_host(self.h, host_ptr, n), "ww_test_prps_host")
 
     def sync(self, timeout_ms: int = 600_000):
         check(_L.ww_sync(self.h, timeout_ms), "ww_sync")
