@@ -92,6 +92,9 @@ int wallsunsun_grid() {
 
 }  // namespace
 
+int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime, uint64_t *g_invert,
+                 uint32_t *primecount, uint64_t capacity, uint32_t *overflow, void *stream, u64 *cursor);
+
 extern "C" {
 
 const char *ww_last_error(void) { return g_err; }
@@ -137,6 +140,15 @@ int ww_launch_clearresult(uint64_t *checksum, uint32_t *resultcount, uint64_t *t
 int ww_launch_getsegprimes(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime,
                            uint64_t *g_invert, uint32_t *primecount, uint64_t capacity,
                            uint32_t *overflow, void *stream) {
+    return launch_sieve(low, high, wheelidx, g_prime, g_invert, primecount, capacity, overflow, stream, nullptr);
+}
+
+}  // extern "C"
+
+// The sieve launch; with a segment cursor (zeroed here, on the stream) the
+// CTAs take segments dynamically instead of striding.
+int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime, uint64_t *g_invert,
+                 uint32_t *primecount, uint64_t capacity, uint32_t *overflow, void *stream, u64 *cursor) {
     if (!g_prime || !g_invert || !primecount || !overflow) return set_err("null pointer"), WW_ERR_ARG;
     if (low < 127 || high <= low) return set_err("bad range [%llu, %llu)", (unsigned long long)low,
                                                   (unsigned long long)high), WW_ERR_ARG;
@@ -156,10 +168,13 @@ int ww_launch_getsegprimes(uint64_t low, uint64_t high, int32_t wheelidx, uint64
     const uint64_t slots = (uint64_t)sm_count() * (uint64_t)per_sm;
     const uint64_t grid = nseg < slots ? nseg : slots;
     PrpOut out{(u64 *)g_prime, (u64 *)g_invert, primecount, capacity, overflow};
-    k_sieve_prp<<<(unsigned)grid, kSieveThreads, 0, as_stream(stream)>>>(low, high, nseg, out);
+    if (cursor) WW_CU(cudaMemsetAsync(cursor, 0, sizeof(u64), as_stream(stream)));
+    k_sieve_prp<<<(unsigned)grid, kSieveThreads, 0, as_stream(stream)>>>(low, high, nseg, out, cursor);
     WW_CHECK_LAUNCH();
     return WW_OK;
 }
+
+extern "C" {
 
 int ww_launch_wieferich(uint32_t *primecount, const uint64_t *g_prime, const uint64_t *g_invert,
                         uint64_t *g_one, uint64_t *special_prime, int32_t *rem, int32_t *quot,
@@ -203,7 +218,7 @@ int ww_launch_test_prps(uint32_t *primecount, const uint64_t *g_prime, const uin
     HitOut h{(u64 *)special_prime, rem, quot, result, resultcount, numresults, overflow};
     k_test_prps<<<test_grid(), kTestThreads, 0, as_stream(stream)>>>(
         primecount, (const u64 *)g_prime, (const u64 *)g_invert, h, (u64 *)checksum,
-        (u64 *)totalprimecount, capacity);
+        (u64 *)totalprimecount, capacity, nullptr);
     WW_CHECK_LAUNCH();
     return WW_OK;
 }
@@ -261,6 +276,7 @@ struct ww_ctx {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copied[2] = {}, consumed[2] = {};
     u32 *d_chunk = nullptr, *h_chunk = nullptr;  // [2 * kHostChunksMax]: count, max
+    u64 *d_cursor = nullptr;  // work cursors: [0] ww_test_prps, [1] ww_sieve_prp, [2 + i] host chunk i
 };
 
 namespace {
@@ -282,6 +298,7 @@ int ww_open(int device, ww_ctx **out) {
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->dc, sizeof(DevCounters));
     if (e == cudaSuccess) e = cudaMallocHost(&c->hc, sizeof(DevCounters));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_cursor, (2 + kHostChunksMax) * sizeof(u64));
     for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->dc, 0, sizeof(DevCounters), c->stream);
     if (e != cudaSuccess) {
@@ -307,6 +324,7 @@ void ww_close(ww_ctx *c) {
     cudaFree(c->hquot);
     cudaFree(c->hres);
     cudaFree(c->dc);
+    cudaFree(c->d_cursor);
     if (c->hc) cudaFreeHost(c->hc);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     cudaFree(c->d_chunk);
@@ -407,8 +425,8 @@ int ww_clear_segment(ww_ctx *c) {
 
 int ww_sieve_prp(ww_ctx *c, uint64_t kernel_start, uint64_t stop, int32_t wheel_idx) {
     WW_NEED_BUFFERS(c);
-    return ww_launch_getsegprimes(kernel_start, stop, wheel_idx, (uint64_t *)c->prime, (uint64_t *)c->inv, c->dc->primecount,
-                                  c->cap, &c->dc->overflow, c->stream);
+    return launch_sieve(kernel_start, stop, wheel_idx, (uint64_t *)c->prime, (uint64_t *)c->inv, c->dc->primecount,
+                        c->cap, &c->dc->overflow, c->stream, c->d_cursor + 1);
 }
 
 int ww_wieferich(ww_ctx *c) {
@@ -429,10 +447,13 @@ int ww_wallsunsun(ww_ctx *c) {
 
 int ww_test_prps(ww_ctx *c) {
     WW_NEED_BUFFERS(c);
-    return ww_launch_test_prps(c->dc->primecount, (uint64_t *)c->prime, (uint64_t *)c->inv, (uint64_t *)c->hprime,
-                               c->hrem, c->hquot, c->hres, (uint64_t *)&c->dc->checksum, &c->dc->resultcount,
-                               (uint64_t *)&c->dc->total, c->cap, c->hcap,
-                               &c->dc->overflow, c->stream);
+    WW_CU(cudaMemsetAsync(c->d_cursor, 0, sizeof(u64), c->stream));
+    HitOut h{c->hprime, c->hrem, c->hquot, c->hres, &c->dc->resultcount, c->hcap, &c->dc->overflow};
+    k_test_prps<<<test_grid(), kTestThreads, 0, c->stream>>>(c->dc->primecount, c->prime, c->inv, h,
+                                                             (u64 *)&c->dc->checksum, (u64 *)&c->dc->total,
+                                                             c->cap, c->d_cursor);
+    WW_CHECK_LAUNCH();
+    return WW_OK;
 }
 
 int ww_load_prps(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
@@ -483,6 +504,7 @@ int ww_test_prps_host(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
         c->h_chunk[2 * i + 1] = 0;
     }
     WW_CU(cudaMemcpyAsync(c->d_chunk, c->h_chunk, 2 * nchunks * sizeof(u32), cudaMemcpyHostToDevice, c->stream));
+    WW_CU(cudaMemsetAsync(c->d_cursor + 2, 0, nchunks * sizeof(u64), c->stream));
     // the copy stream must not overwrite a half that earlier test work still reads
     WW_CU(cudaEventRecord(c->consumed[0], c->stream));
     WW_CU(cudaEventRecord(c->consumed[1], c->stream));
@@ -497,7 +519,7 @@ int ww_test_prps_host(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
         WW_CU(cudaStreamWaitEvent(c->stream, c->copied[half], 0));
         k_test_prps<<<test_grid(), kTestThreads, 0, c->stream>>>(c->d_chunk + 2 * i, dst, nullptr, h,
                                                                  (u64 *)&c->dc->checksum, (u64 *)&c->dc->total,
-                                                                 len);
+                                                                 len, c->d_cursor + 2 + i);
         WW_CHECK_LAUNCH();
         WW_CU(cudaEventRecord(c->consumed[half], c->stream));
     }

@@ -20,17 +20,27 @@ namespace ww {
 
 // Sieve + SPRP over [lo, hi).  b0 = lo & ~1; segment s holds the odd numbers
 // b0 + 2(s*kSegOdd + j) + 1, j < kSegOdd.
-__global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out) {
+// With a segment cursor (zeroed before the launch) the CTAs take segments
+// one at a time from it; without one (the kernel-shaped entry point) they
+// stride over the segments.
+__global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out, u64 *cursor) {
     __shared__ u32 bitmap[kSegWords];
     __shared__ u32 queue[kSieveWarps][kQueueCap];
     __shared__ u32 rescue[kRescueCap];
     __shared__ u32 rescue_n, s_chunk;
+    __shared__ u64 s_seg;
     const u64 b0 = lo & ~1ull;
     const u64 span = hi - b0;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
 
-    for (u64 seg = blockIdx.x; seg < nseg; seg += gridDim.x) {
+    u64 seg = blockIdx.x;
+    if (cursor) {
+        if (threadIdx.x == 0) s_seg = atomicAdd((unsigned long long *)cursor, 1ull);
+        __syncthreads();
+        seg = s_seg;
+    }
+    while (seg < nseg) {
         const u64 seg_off = seg * (u64)(2 * kSegOdd);
         const u64 rem_span = span - seg_off;  // > 0
         const u64 nvalid = (rem_span / 2 < (u64)kSegOdd) ? rem_span / 2 : (u64)kSegOdd;
@@ -115,6 +125,13 @@ __global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64
             if (!more) break;
         }
         __syncthreads();  // bitmap reused by the next segment
+        if (cursor) {
+            if (threadIdx.x == 0) s_seg = atomicAdd((unsigned long long *)cursor, 1ull);
+            __syncthreads();
+            seg = s_seg;
+        } else {
+            seg += gridDim.x;
+        }
     }
 }
 
@@ -175,12 +192,20 @@ __global__ void __launch_bounds__(kTestThreads, WW_TEST_MINB) k_wallsunsun(const
     if ((threadIdx.x & 31) == 0 && sum) atomicAdd(checksum, sum);
 }
 
+// Primes a warp takes per fetch from the work cursor (8 per lane).
+constexpr u64 kWarpFetch = 256;
+
+// Both tests over the list.  With a work cursor (zeroed before the launch)
+// each warp pulls kWarpFetch primes at a time, so warps that run ahead take
+// more of the list and all finish together; without one (the kernel-shaped
+// entry point, which has no scratch) the grid strides over the list.
 __global__ void __launch_bounds__(kTestThreads, WW_TEST_MINB) k_test_prps(u32 *primecount, const u64 *prime,
                                                              const u64 *inv, HitOut hits, u64 *checksum,
-                                                             u64 *totalprimecount, u64 capacity) {
+                                                             u64 *totalprimecount, u64 capacity,
+                                                             u64 *cursor) {
     const u64 n = min((u64)primecount[0], capacity);
     u64 sum = 0;
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+    auto test_one = [&](u64 i) {
         const u64 p = prime[i];
         const u64 q = inv ? inv[i] : inv64(p);
         const D2 one = m2_one(p);
@@ -190,6 +215,20 @@ __global__ void __launch_bounds__(kTestThreads, WW_TEST_MINB) k_test_prps(u32 *p
         int rem, quot, res;
         if (wieferich_classify(p, s, rem, quot)) emit_hit(hits, p, 1093, rem, quot);
         if (wss_classify(p, c, res, quot)) emit_hit(hits, p, res, 0, quot);
+    };
+    if (cursor) {
+        const int lane = threadIdx.x & 31;
+        for (;;) {
+            u64 base = 0;
+            if (lane == 0) base = atomicAdd((unsigned long long *)cursor, (unsigned long long)kWarpFetch);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= n) break;
+            const u64 end = min(base + kWarpFetch, n);
+            for (u64 i = base + lane; i < end; i += 32) test_one(i);
+        }
+    } else {
+        for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+            test_one(i);
     }
     sum = warp_sum(sum);
     if ((threadIdx.x & 31) == 0 && sum) atomicAdd(checksum, sum);
