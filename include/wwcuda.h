@@ -355,8 +355,10 @@ int ww_selftest_range(uint64_t lo, uint64_t hi, uint64_t *prp_count, uint64_t *c
  * case, out = (z0, z1). */
 int ww_selftest_m2(int op, uint64_t p, const uint64_t *xy, uint64_t n, uint64_t *out);
 /* The kernels' PRP-test candidates of [lo, hi) computed on the host
- * (small primes 3..113, then the deep sieve to 2^16 with its rescue list of
- * possible base-2 pseudoprimes), sorted; *rescued = rescue-list length. */
+ * (small primes 3..113, then the deep sieve, which leaves unmarked every
+ * multiple r*k with k = 1 (mod ord_r(2)): r itself and every possible
+ * base-2 pseudoprime with the factor r), sorted; *rescued = the number of
+ * deep-prime multiples left unmarked that way. */
 int ww_selftest_candidates(uint64_t lo, uint64_t hi, uint64_t *out, uint64_t cap, uint64_t *n,
                            uint64_t *rescued);
 

@@ -162,8 +162,8 @@ def test_m2_arithmetic_random(ww):
 @pytest.mark.parametrize("lo,hi", [(127, 2_000_000), (1_373_553, 4_373_653), (2**32 - 10**6, 2**32 + 10**6),
                                    (2**64 - 2 * 10**6 - 1, 2**64 - 1), (10**15, 10**15 + 3_000_000)])
 def test_deep_sieve_keeps_every_prp(ww, oracle, lo, hi):
-    """The deep sieve (primes to 2^16) with its rescue list of possible
-    base-2 pseudoprimes keeps every PRP of the reference's definition, and
+    """The deep sieve (primes to 2^20), which spares every multiple r*k with
+    k = 1 (mod ord_r(2)), keeps every PRP of the reference's definition, and
     only numbers with no factor <= 113 reach the PRP test."""
     cand, rescued = ww.selftest_candidates(lo, hi)
     summ, prps, _ = oracle.scan_range(lo, hi, want_prps=True, prp_cap=(hi - lo) // 2 + 8)
@@ -180,14 +180,13 @@ def test_deep_sieve_keeps_every_prp(ww, oracle, lo, hi):
         assert n in set(cand.tolist())
 
 
-def test_deep_sieve_rescues_pseudoprimes_with_deep_factors(ww, oracle):
+def test_deep_sieve_spares_pseudoprimes_with_deep_factors(ww, oracle):
     # 49141 = 157 * 313 and 88357 = 149 * 593 are base-2 strong pseudoprimes
-    # whose factors are deep-sieve primes: only the rescue list keeps them
+    # whose factors are deep-sieve primes: only the cofactor rule keeps them
     for n in (49141, 88357, 104653):
         assert oracle.is_prp(n) and not oracle.is_prime(n)
         cand, rescued = ww.selftest_candidates(n - 2000, n + 2000)
         assert cand.tolist().count(n) == 1 and rescued >= 1
-    # 49141 sits in the rescue classes of both its factors; it is listed
-    # twice but must reach the PRP test once
+    # 49141 is spared by both of its factors; it must reach the PRP test once
     cand, rescued = ww.selftest_candidates(49141 - 10, 49141 + 10)
     assert rescued >= 2 and cand.tolist().count(49141) == 1

@@ -1,13 +1,21 @@
-"""Generate ww_deep_table.h: the primes 127 < r < 2^16 whose multiplicative
-order of 2 is at least 32, with o = ord_r(2), m = r*o and the constants
-2^32 mod r, 2^32 mod m used for 32-bit modular reductions on the device.
+"""Generate ww_deep_table.h: the deep-sieve primes 113 < r < 2^20, one row
+each with o = ord_r(2) and the constants the device uses to start a
+prime's marking in a segment without divisions:
+
+    rinv = r^-1 mod 2^64          (exact quotient n / r of a multiple n)
+    mr   = floor(2^64 / r)        (Barrett reduction of a 64-bit number mod r)
+    mo   = floor(2^64 / o)        (the same mod o)
+
+The rows come in bands: WW_DEEP_ROWS_<b>(X) holds the primes with
+2^(b-1) <= r < 2^b (b = 16 for all r < 2^16), and WW_DEEP_COUNT_<b> counts
+the rows below 2^b, so a build that sieves to 2^B compiles only the bands up
+to B.
 
 Run from the repository root:  python wwocl-boinc_b200/csrc/gen_deep_table.py
 """
 from pathlib import Path
 
-LIMIT = 1 << 16
-MIN_ORDER = 32
+LIMIT_BITS = 20
 
 
 def primes_below(n):
@@ -39,28 +47,28 @@ def order_of_two(r):
 
 def main():
     rows = []
-    for r in primes_below(LIMIT):
+    for r in primes_below(1 << LIMIT_BITS):
         if r <= 113:
             continue
         o = order_of_two(r)
-        if o < MIN_ORDER:
-            continue
-        m = r * o
-        assert m < 2**32
-        rows.append((r, m, (2**32) % r, (2**32) % m))
+        assert o >= 3
+        rows.append((r, o, pow(r, -1, 2**64), 2**64 // r, 2**64 // o))
     out = Path(__file__).resolve().parent / "ww_deep_table.h"
     lines = ["// Generated by gen_deep_table.py -- do not edit.",
-             "// Deep-sieve primes 127 < r < 2^16 with ord_r(2) >= %d, one row each:" % MIN_ORDER,
-             "// X(r, m = r * ord_r(2), 2^32 mod r, 2^32 mod m)",
-             "#pragma once",
-             "#define WW_DEEP_COUNT %d" % len(rows),
-             "#define WW_DEEP_ROWS(X) \\"]
-    for i in range(0, len(rows), 4):
-        lines.append("    " + " ".join("X(%du, %du, %du, %du)" % row for row in rows[i:i + 4]) + " \\")
-    lines.append("")
+             "// Deep-sieve primes 113 < r < 2^%d in bands by bit length, one row each:" % LIMIT_BITS,
+             "// X(r, o = ord_r(2), r^-1 mod 2^64, floor(2^64 / r), floor(2^64 / o))",
+             "#pragma once"]
+    for b in range(16, LIMIT_BITS + 1):
+        lines.append("#define WW_DEEP_COUNT_%d %d" % (b, sum(1 for row in rows if row[0] < (1 << b))))
+    for b in range(16, LIMIT_BITS + 1):
+        band = [row for row in rows if row[0] < (1 << b) and (b == 16 or row[0] >= (1 << (b - 1)))]
+        lines.append("#define WW_DEEP_ROWS_%d(X) \\" % b)
+        for i in range(0, len(band), 2):
+            lines.append("    " + " ".join("X(%du, %du, 0x%016xull, 0x%016xull, 0x%016xull)" % row
+                                           for row in band[i:i + 2]) + " \\")
+        lines.append("")
     out.write_text("\n".join(lines) + "\n")
-    print(len(rows), "primes;", "excluded (small order):",
-          [r for r in primes_below(LIMIT) if r > 113 and order_of_two(r) < MIN_ORDER])
+    print(len(rows), "rows")
 
 
 if __name__ == "__main__":

@@ -123,7 +123,7 @@ __device__ __forceinline__ void test_batch(const u64 *qp, int n_valid, u32 unit,
 template <class Cfg>
 constexpr size_t batch_smem_bytes() {
     return (size_t)Cfg::kWarps * Cfg::kPrpCap * 8 + (size_t)Cfg::kWords * 4 +
-           (size_t)Cfg::kWarps * Cfg::kCandCap * 4 + (size_t)kRescueCap * 4;
+           (size_t)Cfg::kWarps * Cfg::kCandCap * 4;
 }
 
 // Hand out the next tile.  Batch: the global queue head over the static
@@ -166,10 +166,8 @@ __global__ void __launch_bounds__(Cfg::kThreads) k_tiles(BatchArgs a) {
     u32 *bitmap = reinterpret_cast<u32 *>(smem + (size_t)Cfg::kWarps * Cfg::kPrpCap * 8);
     u32(*candq)[Cfg::kCandCap] =
         reinterpret_cast<u32(*)[Cfg::kCandCap]>(smem + (size_t)Cfg::kWarps * Cfg::kPrpCap * 8 + Cfg::kWords * 4);
-    u32 *rescue = reinterpret_cast<u32 *>(smem + (size_t)Cfg::kWarps * Cfg::kPrpCap * 8 + Cfg::kWords * 4 +
-                                          (size_t)Cfg::kWarps * Cfg::kCandCap * 4);
     __shared__ u64 s_lo, s_hi;
-    __shared__ u32 s_unit, s_chunk, s_ok, s_rescue_n;
+    __shared__ u32 s_unit, s_chunk, s_ok;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
 
@@ -178,7 +176,6 @@ __global__ void __launch_bounds__(Cfg::kThreads) k_tiles(BatchArgs a) {
             u32 k = 0;
             u64 t = 0;
             s_chunk = 0;
-            s_rescue_n = 0;
             s_ok = next_tile<SERVE>(a, k, t) ? 1u : 0u;
             if (s_ok) {
                 const UnitState &u = a.units[k];
@@ -221,15 +218,9 @@ __global__ void __launch_bounds__(Cfg::kThreads) k_tiles(BatchArgs a) {
         }
         __syncthreads();
 
-        // ---- deep sieve 127..2^16 with the pseudoprime rescue list
+        // ---- deep sieve 113 < r < 2^WW_DEEP_BITS, sparing possible pseudoprimes
         const u64 nbase = b0 + 1;
-        deep_collect(nbase, (u32)nvalid, bitmap, rescue, &s_rescue_n, threadIdx.x, Cfg::kThreads);
-        __syncthreads();
-        if (s_rescue_n <= (u32)kRescueCap) {  // else: this tile keeps the small-prime sieve only
-            deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, Cfg::kThreads);
-            __syncthreads();
-            deep_unmark(bitmap, rescue, s_rescue_n, threadIdx.x, Cfg::kThreads);
-        }
+        deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, Cfg::kThreads);
         __syncthreads();
 
         // ---- chunks of 32 words, taken dynamically by the warps

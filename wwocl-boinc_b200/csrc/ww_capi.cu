@@ -187,7 +187,7 @@ int ww_launch_wieferich(uint32_t *primecount, const uint64_t *g_prime, const uin
     HitOut h{(u64 *)special_prime, rem, quot, result, resultcount, numresults, overflow};
     k_wieferich<<<wieferich_grid(), kTestThreads, 0, as_stream(stream)>>>(
         primecount, (const u64 *)g_prime, (const u64 *)g_invert, (u64 *)g_one, h, (u64 *)checksum,
-        (u64 *)totalprimecount, capacity);
+        (u64 *)totalprimecount, capacity, nullptr);
     WW_CHECK_LAUNCH();
     return WW_OK;
 }
@@ -203,7 +203,7 @@ int ww_launch_wallsunsun(const uint32_t *primecount, const uint64_t *g_prime,
     HitOut h{(u64 *)special_prime, rem, quot, result, resultcount, numresults, overflow};
     k_wallsunsun<<<wallsunsun_grid(), kTestThreads, 0, as_stream(stream)>>>(
         primecount, (const u64 *)g_prime, (const u64 *)g_invert, (const u64 *)g_one, h,
-        (u64 *)checksum, capacity);
+        (u64 *)checksum, capacity, nullptr);
     WW_CHECK_LAUNCH();
     return WW_OK;
 }
@@ -276,7 +276,8 @@ struct ww_ctx {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copied[2] = {}, consumed[2] = {};
     u32 *d_chunk = nullptr, *h_chunk = nullptr;  // [2 * kHostChunksMax]: count, max
-    u64 *d_cursor = nullptr;  // work cursors: [0] ww_test_prps, [1] ww_sieve_prp, [2 + i] host chunk i
+    u64 *d_cursor = nullptr;  // work cursors: [0] ww_test_prps, [1] ww_sieve_prp, [2] ww_wieferich,
+                              // [3] ww_wallsunsun, [4 + i] host chunk i
 };
 
 namespace {
@@ -298,7 +299,7 @@ int ww_open(int device, ww_ctx **out) {
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->dc, sizeof(DevCounters));
     if (e == cudaSuccess) e = cudaMallocHost(&c->hc, sizeof(DevCounters));
-    if (e == cudaSuccess) e = cudaMalloc(&c->d_cursor, (2 + kHostChunksMax) * sizeof(u64));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_cursor, (4 + kHostChunksMax) * sizeof(u64));
     for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->dc, 0, sizeof(DevCounters), c->stream);
     if (e != cudaSuccess) {
@@ -431,18 +432,24 @@ int ww_sieve_prp(ww_ctx *c, uint64_t kernel_start, uint64_t stop, int32_t wheel_
 
 int ww_wieferich(ww_ctx *c) {
     WW_NEED_BUFFERS(c);
-    return ww_launch_wieferich(c->dc->primecount, (uint64_t *)c->prime, (uint64_t *)c->inv, (uint64_t *)c->one,
-                               (uint64_t *)c->hprime, c->hrem, c->hquot, c->hres, (uint64_t *)&c->dc->checksum,
-                               &c->dc->resultcount, (uint64_t *)&c->dc->total, c->cap,
-                               c->hcap, &c->dc->overflow, c->stream);
+    WW_CU(cudaMemsetAsync(c->d_cursor + 2, 0, sizeof(u64), c->stream));
+    HitOut h{c->hprime, c->hrem, c->hquot, c->hres, &c->dc->resultcount, c->hcap, &c->dc->overflow};
+    k_wieferich<<<wieferich_grid(), kTestThreads, 0, c->stream>>>(c->dc->primecount, c->prime, c->inv, c->one, h,
+                                                                  (u64 *)&c->dc->checksum, (u64 *)&c->dc->total,
+                                                                  c->cap, c->d_cursor + 2);
+    WW_CHECK_LAUNCH();
+    return WW_OK;
 }
 
 int ww_wallsunsun(ww_ctx *c) {
     WW_NEED_BUFFERS(c);
-    return ww_launch_wallsunsun(c->dc->primecount, (uint64_t *)c->prime, (uint64_t *)c->inv, (uint64_t *)c->one,
-                                (uint64_t *)c->hprime, c->hrem, c->hquot, c->hres, (uint64_t *)&c->dc->checksum,
-                                &c->dc->resultcount, c->cap, c->hcap,
-                                &c->dc->overflow, c->stream);
+    WW_CU(cudaMemsetAsync(c->d_cursor + 3, 0, sizeof(u64), c->stream));
+    HitOut h{c->hprime, c->hrem, c->hquot, c->hres, &c->dc->resultcount, c->hcap, &c->dc->overflow};
+    k_wallsunsun<<<wallsunsun_grid(), kTestThreads, 0, c->stream>>>(c->dc->primecount, c->prime, c->inv, c->one, h,
+                                                                    (u64 *)&c->dc->checksum, c->cap,
+                                                                    c->d_cursor + 3);
+    WW_CHECK_LAUNCH();
+    return WW_OK;
 }
 
 int ww_test_prps(ww_ctx *c) {
@@ -504,7 +511,7 @@ int ww_test_prps_host(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
         c->h_chunk[2 * i + 1] = 0;
     }
     WW_CU(cudaMemcpyAsync(c->d_chunk, c->h_chunk, 2 * nchunks * sizeof(u32), cudaMemcpyHostToDevice, c->stream));
-    WW_CU(cudaMemsetAsync(c->d_cursor + 2, 0, nchunks * sizeof(u64), c->stream));
+    WW_CU(cudaMemsetAsync(c->d_cursor + 4, 0, nchunks * sizeof(u64), c->stream));
     // the copy stream must not overwrite a half that earlier test work still reads
     WW_CU(cudaEventRecord(c->consumed[0], c->stream));
     WW_CU(cudaEventRecord(c->consumed[1], c->stream));
@@ -519,7 +526,7 @@ int ww_test_prps_host(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
         WW_CU(cudaStreamWaitEvent(c->stream, c->copied[half], 0));
         k_test_prps<<<test_grid(), kTestThreads, 0, c->stream>>>(c->d_chunk + 2 * i, dst, nullptr, h,
                                                                  (u64 *)&c->dc->checksum, (u64 *)&c->dc->total,
-                                                                 len, c->d_cursor + 2 + i);
+                                                                 len, c->d_cursor + 4 + i);
         WW_CHECK_LAUNCH();
         WW_CU(cudaEventRecord(c->consumed[half], c->stream));
     }

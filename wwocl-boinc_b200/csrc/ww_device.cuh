@@ -88,56 +88,41 @@ __device__ __forceinline__ void step_hit(u32 &j0) {
 // ------------------------------------------------------------- deep sieve
 // (the scheme is described in ww_deep.cuh)
 
-#define WW_DEEP_ROW4(r, m, a, b) {r, m, a, b},
-static __device__ const uint4 kDeepDev[WW_DEEP_COUNT] = {WW_DEEP_ROWS(WW_DEEP_ROW4)};
+#define WW_DEEP_ROWD(r, o, rinv, mr, mo) {r, o, rinv, mr, mo},
+static __device__ const DeepRow kDeepDev[WW_DEEP_COUNT] = {WW_DEEP_ROWS(WW_DEEP_ROWD)};
+#undef WW_DEEP_ROWD
 
-// Rescue list of one segment, built from the small-prime bitmap before the
-// deep marking: bit indices j (odd number first + 2j) of multiples n = r
-// (mod r * ord_r(2)) that have no factor <= 113.  The count may exceed
-// kRescueCap; the caller then skips the deep marking for that segment.
-__device__ __forceinline__ void deep_collect(u64 first, u32 nvalid, const u32 *bitmap, u32 *rescue,
-                                             u32 *rescue_n, int tid, int nthreads) {
-    for (int i = tid; i < WW_DEEP_COUNT; i += nthreads) {
-        const uint4 e = kDeepDev[i];
-        const u64 step = deep_rescue_step(e.y);
-        for (u64 off = deep_first_rescue(first, e.x, e.y, e.w); (off >> 1) < nvalid; off += step) {
-            const u32 j = (u32)(off >> 1);
-            if (!((bitmap[j >> 5] >> (j & 31)) & 1u)) {
-                const u32 k = atomicAdd(rescue_n, 1u);
-                if (k < kRescueCap) rescue[k] = j;
-            }
-        }
-    }
-}
-
-// Clear the rescued bits again once the deep marking is complete, so they
-// reach the PRP test through the bitmap like any survivor.  A number in two
-// rescue classes (a pseudoprime with two deep factors) is listed twice and
-// cleared twice: it is still tested once.
-__device__ __forceinline__ void deep_unmark(u32 *bitmap, const u32 *rescue, u32 nresc, int tid, int nthreads) {
-    for (u32 i = tid; i < nresc; i += nthreads) {
-        const u32 j = rescue[i];
-        atomicAnd(&bitmap[j >> 5], ~(1u << (j & 31)));
-    }
-}
-
-// Mark every odd multiple of the deep primes in the segment.  The smallest
+// Mark the odd multiples n = r*k of the deep primes in the segment, except
+// those with k = 1 (mod ord_r(2)) (ww_deep.cuh says why).  The smallest
 // primes have the most multiples: each of the first kDeepWarpPrimes primes
-// is marked by a whole warp (lane l takes every 32nd multiple), the rest one
-// prime per thread, so no thread holds the others at the next barrier.
+// is marked by a whole warp (lane l takes the multiples l, l + 32, ...; k
+// then grows by 64 per step), the rest one prime per thread, so no thread
+// holds the others at the next barrier.
 constexpr int kDeepWarpPrimes = 512;
 
 __device__ __forceinline__ void deep_mark(u64 first, u32 nvalid, u32 *bitmap, int tid, int nthreads) {
     const int lane = tid & 31, warp = tid >> 5, nwarps = nthreads >> 5;
-    for (int i = warp; i < kDeepWarpPrimes; i += nwarps) {
-        const uint4 e = kDeepDev[i];
-        const u32 j0 = deep_first_multiple(first, e.x, e.z);
-        for (u32 j = j0 + (u32)lane * e.x; j < nvalid; j += 32u * e.x) atomicOr(&bitmap[j >> 5], 1u << (j & 31));
+    for (int i = warp; i < kDeepWarpPrimes && i < kDeepUse; i += nwarps) {
+        const DeepRow e = kDeepDev[i];
+        u32 j0, km0;
+        deep_start(first, e, j0, km0);
+        u32 km = (km0 + 2u * (u32)lane) % e.o;
+        const u32 step = 64u % e.o;
+        for (u32 j = j0 + (u32)lane * e.r; j < nvalid; j += 32u * e.r) {
+            if (km != 1u) atomicOr(&bitmap[j >> 5], 1u << (j & 31));
+            km += step;
+            if (km >= e.o) km -= e.o;
+        }
     }
-    for (int i = kDeepWarpPrimes + tid; i < WW_DEEP_COUNT; i += nthreads) {
-        const uint4 e = kDeepDev[i];
-        for (u32 j = deep_first_multiple(first, e.x, e.z); j < nvalid; j += e.x)
-            atomicOr(&bitmap[j >> 5], 1u << (j & 31));
+    for (int i = kDeepWarpPrimes + tid; i < kDeepUse; i += nthreads) {
+        const DeepRow e = kDeepDev[i];
+        u32 j, km;
+        deep_start(first, e, j, km);
+        for (; j < nvalid; j += e.r) {
+            if (km != 1u) atomicOr(&bitmap[j >> 5], 1u << (j & 31));
+            km += 2u;
+            if (km >= e.o) km -= e.o;
+        }
     }
 }
 

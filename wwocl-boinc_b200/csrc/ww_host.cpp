@@ -262,14 +262,15 @@ extern "C" int ww_selftest_m2(int op, uint64_t p, const uint64_t *xy, uint64_t n
 
 // ---------------------------------------------------------------------------
 // Host emulation of the kernels' candidate generation (small primes 3..113,
-// then the deep sieve with its pseudoprime rescue list), one segment over
-// [lo, hi), for checking that the candidate set keeps every PRP.
+// then the deep sieve that spares multiples r*k with k = 1 (mod ord_r(2))),
+// one segment over [lo, hi), for checking that the candidate set keeps every
+// PRP.
 
 #include "ww_deep.cuh"
 
 namespace {
-#define WW_DEEP_ROWH(r, m, a, b) {r, m, a, b},
-const u32 kDeepHost[WW_DEEP_COUNT][4] = {WW_DEEP_ROWS(WW_DEEP_ROWH)};
+#define WW_DEEP_ROWH(r, o, rinv, mr, mo) {r, o, rinv, mr, mo},
+const DeepRow kDeepHost[WW_DEEP_COUNT] = {WW_DEEP_ROWS(WW_DEEP_ROWH)};
 #undef WW_DEEP_ROWH
 }  // namespace
 
@@ -280,27 +281,27 @@ extern "C" int ww_selftest_candidates(uint64_t lo, uint64_t hi, uint64_t *out, u
     const u64 nvalid = (hi - b0) / 2;
     std::vector<u32> bitmap((nvalid + 31) / 32, 0);
     auto mark = [&](u64 j) { bitmap[j >> 5] |= 1u << (j & 31); };
-    auto marked = [&](u64 j) { return (bitmap[j >> 5] >> (j & 31)) & 1u; };
     static const u32 small[29] = {3,  5,  7,  11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53,
                                   59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113};
     for (u32 r : small)
         for (u64 j = deep_first_multiple(first, r, (u32)((1ull << 32) % r)); j < nvalid; j += r) mark(j);
-    std::vector<u64> rescue;
-    for (int i = 0; i < WW_DEEP_COUNT; ++i) {
-        const u32 *e = kDeepHost[i];
-        for (u64 off = deep_first_rescue(first, e[0], e[1], e[3]); (off >> 1) < nvalid; off += deep_rescue_step(e[1]))
-            if (!marked(off >> 1)) rescue.push_back(off >> 1);
+    u64 spared = 0;  // multiples of deep primes left unmarked (k = 1 mod o)
+    for (int i = 0; i < kDeepUse; ++i) {
+        const DeepRow &e = kDeepHost[i];
+        u32 j0, km;
+        deep_start(first, e, j0, km);
+        for (u64 j = j0; j < nvalid; j += e.r) {
+            if (km != 1u) mark(j);
+            else ++spared;
+            km += 2u;
+            if (km >= e.o) km -= e.o;
+        }
     }
-    for (int i = 0; i < WW_DEEP_COUNT; ++i) {
-        const u32 *e = kDeepHost[i];
-        for (u64 j = deep_first_multiple(first, e[0], e[2]); j < nvalid; j += e[0]) mark(j);
-    }
-    for (u64 j : rescue) bitmap[j >> 5] &= ~(1u << (j & 31));  // as deep_unmark does
     std::vector<u64> cand;
     for (u64 j = 0; j < nvalid; ++j)
-        if (!marked(j)) cand.push_back(first + 2 * j);
+        if (!((bitmap[j >> 5] >> (j & 31)) & 1u)) cand.push_back(first + 2 * j);
     *n = cand.size();
-    if (rescued) *rescued = rescue.size();
+    if (rescued) *rescued = spared;
     for (u64 i = 0; i < cap && i < cand.size(); ++i) out[i] = cand[i];
     return WW_OK;
 }

@@ -26,8 +26,7 @@ namespace ww {
 __global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out, u64 *cursor) {
     __shared__ u32 bitmap[kSegWords];
     __shared__ u32 queue[kSieveWarps][kQueueCap];
-    __shared__ u32 rescue[kRescueCap];
-    __shared__ u32 rescue_n, s_chunk;
+    __shared__ u32 s_chunk;
     __shared__ u64 s_seg;
     const u64 b0 = lo & ~1ull;
     const u64 span = hi - b0;
@@ -67,21 +66,12 @@ __global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64
                 bitmap[w] = m;
             }
         }
-        if (threadIdx.x == 0) {
-            rescue_n = 0;
-            s_chunk = 0;
-        }
+        if (threadIdx.x == 0) s_chunk = 0;
         __syncthreads();
 
-        // ---- deep sieve 127..2^16 with the pseudoprime rescue list
+        // ---- deep sieve 113 < r < 2^WW_DEEP_BITS, sparing possible pseudoprimes
         const u64 nbase = b0 + seg_off + 1;
-        deep_collect(nbase, (u32)nvalid, bitmap, rescue, &rescue_n, threadIdx.x, kSieveThreads);
-        __syncthreads();
-        if (rescue_n <= (u32)kRescueCap) {  // else: this segment keeps the small-prime sieve only
-            deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, kSieveThreads);
-            __syncthreads();
-            deep_unmark(bitmap, rescue, rescue_n, threadIdx.x, kSieveThreads);
-        }
+        deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, kSieveThreads);
         __syncthreads();
 
         // ---- warps take 32-word chunks dynamically (so they reach the next
@@ -144,13 +134,39 @@ __device__ __forceinline__ void count_update(u32 *primecount, u64 *totalprimecou
     if (pc > primecount[1]) primecount[1] = pc;
 }
 
+// Primes a warp takes per fetch from the work cursor: one per lane, so a
+// short list still spreads over every warp and the last fetch of a launch
+// is one prime per lane.
+constexpr u64 kWarpFetch = 32;
+
+// Runs f(i) for every list index i < n.  With a work cursor (zeroed before
+// the launch) each warp pulls kWarpFetch indices at a time, so warps that run
+// ahead take more of the list and all finish together; without one (the
+// kernel-shaped entry points, which have no scratch) the grid strides.
+template <class F>
+__device__ __forceinline__ void for_each_prime(u64 n, u64 *cursor, F &&f) {
+    if (cursor) {
+        const int lane = threadIdx.x & 31;
+        for (;;) {
+            u64 base = 0;
+            if (lane == 0) base = atomicAdd((unsigned long long *)cursor, (unsigned long long)kWarpFetch);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= n) break;
+            const u64 end = min(base + kWarpFetch, n);
+            for (u64 i = base + lane; i < end; i += 32) f(i);
+        }
+    } else {
+        for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) f(i);
+    }
+}
+
 __global__ void __launch_bounds__(kTestThreads, WW_TEST_MINB) k_wieferich(u32 *primecount, const u64 *prime,
                                                              const u64 *inv, u64 *g_one, HitOut hits,
                                                              u64 *checksum, u64 *totalprimecount,
-                                                             u64 capacity) {
+                                                             u64 capacity, u64 *cursor) {
     const u64 n = min((u64)primecount[0], capacity);
     u64 sum = 0;
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+    for_each_prime(n, cursor, [&](u64 i) {
         const u64 p = prime[i];
         const u64 q = inv ? inv[i] : inv64(p);
         const D2 one = m2_one(p);
@@ -162,7 +178,7 @@ __global__ void __launch_bounds__(kTestThreads, WW_TEST_MINB) k_wieferich(u32 *p
         sum += s.d1 & 0xffffffffull;
         int rem, quot;
         if (wieferich_classify(p, s, rem, quot)) emit_hit(hits, p, 1093, rem, quot);
-    }
+    });
     sum = warp_sum(sum);
     if ((threadIdx.x & 31) == 0 && sum) atomicAdd(checksum, sum);
     if (blockIdx.x == 0 && threadIdx.x == 0) count_update(primecount, totalprimecount);
@@ -170,10 +186,11 @@ __global__ void __launch_bounds__(kTestThreads, WW_TEST_MINB) k_wieferich(u32 *p
 
 __global__ void __launch_bounds__(kTestThreads, WW_TEST_MINB) k_wallsunsun(const u32 *primecount, const u64 *prime,
                                                               const u64 *inv, const u64 *g_one,
-                                                              HitOut hits, u64 *checksum, u64 capacity) {
+                                                              HitOut hits, u64 *checksum, u64 capacity,
+                                                              u64 *cursor) {
     const u64 n = min((u64)primecount[0], capacity);
     u64 sum = 0;
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+    for_each_prime(n, cursor, [&](u64 i) {
         const u64 p = prime[i];
         const u64 q = inv ? inv[i] : inv64(p);
         D2 one;
@@ -187,25 +204,19 @@ __global__ void __launch_bounds__(kTestThreads, WW_TEST_MINB) k_wallsunsun(const
         sum += c.d1 & 0xffffffffull;
         int res, quot;
         if (wss_classify(p, c, res, quot)) emit_hit(hits, p, res, 0, quot);
-    }
+    });
     sum = warp_sum(sum);
     if ((threadIdx.x & 31) == 0 && sum) atomicAdd(checksum, sum);
 }
 
-// Primes a warp takes per fetch from the work cursor (8 per lane).
-constexpr u64 kWarpFetch = 256;
-
-// Both tests over the list.  With a work cursor (zeroed before the launch)
-// each warp pulls kWarpFetch primes at a time, so warps that run ahead take
-// more of the list and all finish together; without one (the kernel-shaped
-// entry point, which has no scratch) the grid strides over the list.
+// Both tests over the list in one pass.
 __global__ void __launch_bounds__(kTestThreads, WW_TEST_MINB) k_test_prps(u32 *primecount, const u64 *prime,
                                                              const u64 *inv, HitOut hits, u64 *checksum,
                                                              u64 *totalprimecount, u64 capacity,
                                                              u64 *cursor) {
     const u64 n = min((u64)primecount[0], capacity);
     u64 sum = 0;
-    auto test_one = [&](u64 i) {
+    for_each_prime(n, cursor, [&](u64 i) {
         const u64 p = prime[i];
         const u64 q = inv ? inv[i] : inv64(p);
         const D2 one = m2_one(p);
@@ -215,21 +226,7 @@ __global__ void __launch_bounds__(kTestThreads, WW_TEST_MINB) k_test_prps(u32 *p
         int rem, quot, res;
         if (wieferich_classify(p, s, rem, quot)) emit_hit(hits, p, 1093, rem, quot);
         if (wss_classify(p, c, res, quot)) emit_hit(hits, p, res, 0, quot);
-    };
-    if (cursor) {
-        const int lane = threadIdx.x & 31;
-        for (;;) {
-            u64 base = 0;
-            if (lane == 0) base = atomicAdd((unsigned long long *)cursor, (unsigned long long)kWarpFetch);
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (base >= n) break;
-            const u64 end = min(base + kWarpFetch, n);
-            for (u64 i = base + lane; i < end; i += 32) test_one(i);
-        }
-    } else {
-        for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
-            test_one(i);
-    }
+    });
     sum = warp_sum(sum);
     if ((threadIdx.x & 31) == 0 && sum) atomicAdd(checksum, sum);
     if (blockIdx.x == 0 && threadIdx.x == 0) count_update(primecount, totalprimecount);
