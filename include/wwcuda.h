@@ -340,6 +340,12 @@ int ww_state_read(const char *file_a, const char *file_b, uint64_t start, uint64
  * PRP buffers (replaces primesieve_count_primes, main.cpp:1087-1091). */
 uint64_t ww_prp_count_bound(uint64_t lo, uint64_t hi);
 
+/* Exact number of base-2 strong PRPs with no factor <= 113 in [lo, hi),
+ * lo >= 127, counted on the GPU by the sieve kernel without listing them
+ * (the count primesieve_count_primes gave the reference for sizing,
+ * main.cpp:1000,1087, with its pseudoprimes included).  Synchronises. */
+int ww_count_prps(ww_ctx *ctx, uint64_t lo, uint64_t hi, uint64_t *count);
+
 /* Host twin of the kernels for the start-up self-test (testKernels,
  * main.cpp:590-738): digits of a list (same layout as ww_launch_digits) and
  * the PRP count, checksum and hit count of [lo, hi).  Never used to produce

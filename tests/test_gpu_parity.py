@@ -113,6 +113,25 @@ def test_hits_match_oracle(ctx, oracle):
     assert sorted(got["hits"]) == sorted(want)
 
 
+def test_count_prps_matches_reference(ctx, ref_ranges):
+    """ww_count_prps (the sieve kernel counting without a list) against the
+    reference's PRP counts, including the 2^34-wide range, which is one full
+    counting piece, and a range that ends at 2^64 - 1."""
+    import json
+    from pathlib import Path
+
+    for name in ("small_3e6", "config1_5e7", "cross_2p32", "near_top_2e6", "top_1e8"):
+        r = ref_ranges[name]
+        assert ctx.count_prps(r["lo"], r["hi"]) == r["prp_count"], name
+    long = json.loads((Path(__file__).resolve().parent / "golden" / "ref_long.json").read_text())["config3"]
+    assert ctx.count_prps(long["lo"], long["hi"]) == long["prp_count"]
+    # split at an odd point: the two counts add up
+    r = ref_ranges["config1_5e7"]
+    mid = 12_345_679
+    assert ctx.count_prps(r["lo"], mid) + ctx.count_prps(mid, r["hi"]) == r["prp_count"]
+    assert ctx.count_prps(2**64 - 3, 2**64 - 1) == 0
+
+
 def test_host_list_pipeline_matches_loaded_list(ww, oracle, ref_terms):
     """ww_test_prps_host (chunked copy/test overlap) against ww_load_prps +
     ww_test_prps and the oracle: checksum, count and hits, over a list that

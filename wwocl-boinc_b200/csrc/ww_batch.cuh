@@ -60,7 +60,7 @@ struct BatchCfg {
     static constexpr int kPpt = PPT;
     static constexpr int kChunks = SEG_WORDS / 32;
     static constexpr u64 kTileNumbers = 64ull * SEG_WORDS;  // integers per tile
-    static constexpr int kCandCap = 640;
+    static constexpr int kCandCap = 416;  // as kQueueCap: 31 carried + at most 378 per 32-word chunk
     static constexpr int kPrpCap = 32 * PPT + 32;
     static_assert(SEG_WORDS % THREADS == 0, "words per thread");
 };

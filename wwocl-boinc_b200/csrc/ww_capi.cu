@@ -140,6 +140,7 @@ int ww_launch_clearresult(uint64_t *checksum, uint32_t *resultcount, uint64_t *t
 int ww_launch_getsegprimes(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime,
                            uint64_t *g_invert, uint32_t *primecount, uint64_t capacity,
                            uint32_t *overflow, void *stream) {
+    if (!g_prime || !g_invert) return set_err("null pointer"), WW_ERR_ARG;
     return launch_sieve(low, high, wheelidx, g_prime, g_invert, primecount, capacity, overflow, stream, nullptr);
 }
 
@@ -149,7 +150,8 @@ int ww_launch_getsegprimes(uint64_t low, uint64_t high, int32_t wheelidx, uint64
 // CTAs take segments dynamically instead of striding.
 int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime, uint64_t *g_invert,
                  uint32_t *primecount, uint64_t capacity, uint32_t *overflow, void *stream, u64 *cursor) {
-    if (!g_prime || !g_invert || !primecount || !overflow) return set_err("null pointer"), WW_ERR_ARG;
+    // g_prime == nullptr: count the PRPs without listing them
+    if ((!g_prime && capacity) || !primecount || !overflow) return set_err("null pointer"), WW_ERR_ARG;
     if (low < 127 || high <= low) return set_err("bad range [%llu, %llu)", (unsigned long long)low,
                                                   (unsigned long long)high), WW_ERR_ARG;
     if (wheel_index_of(low) != wheelidx)
@@ -276,8 +278,9 @@ struct ww_ctx {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copied[2] = {}, consumed[2] = {};
     u32 *d_chunk = nullptr, *h_chunk = nullptr;  // [2 * kHostChunksMax]: count, max
+    u32 *d_count = nullptr;   // ww_count_prps: count, max, overflow
     u64 *d_cursor = nullptr;  // work cursors: [0] ww_test_prps, [1] ww_sieve_prp, [2] ww_wieferich,
-                              // [3] ww_wallsunsun, [4 + i] host chunk i
+                              // [3] ww_wallsunsun, [4] ww_count_prps, [5 + i] host chunk i
 };
 
 namespace {
@@ -299,7 +302,8 @@ int ww_open(int device, ww_ctx **out) {
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->dc, sizeof(DevCounters));
     if (e == cudaSuccess) e = cudaMallocHost(&c->hc, sizeof(DevCounters));
-    if (e == cudaSuccess) e = cudaMalloc(&c->d_cursor, (4 + kHostChunksMax) * sizeof(u64));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_cursor, (5 + kHostChunksMax) * sizeof(u64));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_count, 4 * sizeof(u32));
     for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->dc, 0, sizeof(DevCounters), c->stream);
     if (e != cudaSuccess) {
@@ -326,6 +330,7 @@ void ww_close(ww_ctx *c) {
     cudaFree(c->hres);
     cudaFree(c->dc);
     cudaFree(c->d_cursor);
+    cudaFree(c->d_count);
     if (c->hc) cudaFreeHost(c->hc);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     cudaFree(c->d_chunk);
@@ -511,7 +516,7 @@ int ww_test_prps_host(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
         c->h_chunk[2 * i + 1] = 0;
     }
     WW_CU(cudaMemcpyAsync(c->d_chunk, c->h_chunk, 2 * nchunks * sizeof(u32), cudaMemcpyHostToDevice, c->stream));
-    WW_CU(cudaMemsetAsync(c->d_cursor + 4, 0, nchunks * sizeof(u64), c->stream));
+    WW_CU(cudaMemsetAsync(c->d_cursor + 5, 0, nchunks * sizeof(u64), c->stream));
     // the copy stream must not overwrite a half that earlier test work still reads
     WW_CU(cudaEventRecord(c->consumed[0], c->stream));
     WW_CU(cudaEventRecord(c->consumed[1], c->stream));
@@ -526,9 +531,37 @@ int ww_test_prps_host(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
         WW_CU(cudaStreamWaitEvent(c->stream, c->copied[half], 0));
         k_test_prps<<<test_grid(), kTestThreads, 0, c->stream>>>(c->d_chunk + 2 * i, dst, nullptr, h,
                                                                  (u64 *)&c->dc->checksum, (u64 *)&c->dc->total,
-                                                                 len, c->d_cursor + 4 + i);
+                                                                 len, c->d_cursor + 5 + i);
         WW_CHECK_LAUNCH();
         WW_CU(cudaEventRecord(c->consumed[half], c->stream));
+    }
+    return WW_OK;
+}
+
+int ww_count_prps(ww_ctx *c, uint64_t lo, uint64_t hi, uint64_t *count) {
+    if (!c || !count) return set_err("null argument"), WW_ERR_ARG;
+    if (lo < 127 || hi < lo) return set_err("bad range [%llu, %llu)", (unsigned long long)lo,
+                                            (unsigned long long)hi), WW_ERR_ARG;
+    WW_CU(cudaSetDevice(c->device));
+    *count = 0;
+    // pieces of 2^34 numbers keep every piece's count inside the 32-bit counter
+    constexpr u64 kPiece = 1ull << 34;
+    for (u64 a = lo; a < hi;) {
+        const u64 b = hi - a > kPiece ? a + kPiece : hi;
+        uint64_t ks = a;
+        int32_t idx = 0;
+        if (ww_find_wheel_offset(&ks, &idx) != WW_OK) break;  // nothing prime to 30 is left below 2^64
+        if (ks < b) {
+            WW_CU(cudaMemsetAsync(c->d_count, 0, 4 * sizeof(u32), c->stream));
+            const int rc = launch_sieve(ks, b, idx, nullptr, nullptr, c->d_count, 0, c->d_count + 2, c->stream,
+                                        c->d_cursor + 4);
+            if (rc) return rc;
+            u32 n = 0;
+            WW_CU(cudaMemcpyAsync(&n, c->d_count, sizeof(u32), cudaMemcpyDeviceToHost, c->stream));
+            WW_CU(cudaStreamSynchronize(c->stream));
+            *count += n;
+        }
+        a = b;
     }
     return WW_OK;
 }

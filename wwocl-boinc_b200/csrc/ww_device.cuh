@@ -11,12 +11,16 @@
 
 namespace ww {
 
-constexpr int kSegWords = 4096;               // bitmap words per segment (16 KB)
+constexpr int kSegWords = 8192;               // bitmap words per segment (32 KB, 2^19 numbers)
 constexpr int kSegOdd = kSegWords * 32;       // odd numbers per segment
 constexpr int kSieveThreads = 256;
 constexpr int kSieveWarps = kSieveThreads / 32;
 constexpr int kWordsPerThread = kSegWords / kSieveThreads;
-constexpr int kQueueCap = 640;  // 31 carried + 32 words x at most 18 survivors
+// A warp queue holds the < 32 candidates carried over plus one chunk of 32
+// words (1024 odd numbers).  Among any 1024 consecutive odd numbers at most
+// 378 have no factor 3..17 (the maximum over the full period 3*5*...*17), so
+// 31 + 378 entries always suffice.
+constexpr int kQueueCap = 416;
 #ifndef WW_TEST_THREADS
 #define WW_TEST_THREADS 256
 #endif
@@ -142,7 +146,7 @@ __device__ __forceinline__ void sprp_emit(const PrpOut &out, u64 n, bool active)
     u32 base = 0;
     if (lane == 0) base = atomicAdd(out.count, (u32)__popc(ballot));
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (pass) {
+    if (pass && out.prime) {  // no list: count only
         const u64 ix = (u64)base + (u64)__popc(ballot & ((1u << lane) - 1u));
         if (ix < out.capacity) {
             out.prime[ix] = n;

@@ -114,6 +114,7 @@ _SIGS = {
     "ww_test_prps": (C.c_int, [_VP]),
     "ww_load_prps": (C.c_int, [_VP, _VP, C.c_uint64]),
     "ww_test_prps_host": (C.c_int, [_VP, _VP, C.c_uint64]),
+    "ww_count_prps": (C.c_int, [_VP, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]),
     "ww_marker": (C.c_int, [_VP, C.c_int]),
     "ww_wait_marker": (C.c_int, [_VP, C.c_int, C.c_uint32]),
     "ww_marker_elapsed": (C.c_int, [_VP, C.c_int, C.c_int, C.POINTER(C.c_float)]),
@@ -337,6 +338,12 @@ class Context:
 
     def load_prps_ptr(self, host_ptr: int, n: int) -> None:
         check(_L.ww_load_prps(self.h, host_ptr, n), "ww_load_prps")
+
+    def count_prps(self, lo: int, hi: int) -> int:
+        """Exact PRP count of [lo, hi) from the sieve kernel (no list)."""
+        n = C.c_uint64(0)
+        check(_L.ww_count_prps(self.h, lo, hi, C.byref(n)), "ww_count_prps")
+        return n.value
 
     def test_prps_host(self, primes: np.ndarray) -> None:
         """Both tests over a host list, copy and test pipelined in chunks."""
