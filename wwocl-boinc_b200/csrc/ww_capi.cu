@@ -500,20 +500,22 @@ int ww_test_prps_host(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
         WW_CU(cudaMalloc(&c->d_chunk, 2 * kHostChunksMax * sizeof(u32)));
         WW_CU(cudaMallocHost(&c->h_chunk, 2 * kHostChunksMax * sizeof(u32)));
     }
-    // chunk: about an eighth of the list (at least 2^20 PRPs), at most half
-    // the buffer, and few enough chunks for the count table
-    u64 chunk = std::max<u64>(1ull << 20, (n + 7) / 8);
-    chunk = std::max<u64>(chunk, (n + kHostChunksMax - 1) / kHostChunksMax);
-    chunk = std::min<u64>(chunk, std::min<u64>(c->cap / 2, 0xffffffffull));
-    const u64 nchunks = (n + chunk - 1) / chunk;
-    if (nchunks > kHostChunksMax)
-        return set_err("list of %llu PRPs needs a PRP buffer of at least %llu entries", (unsigned long long)n,
-                       (unsigned long long)(2 * ((n + kHostChunksMax - 1) / kHostChunksMax))), WW_ERR_ARG;
-    // the previous call's kernels may still read the count table
+    // Chunks grow from 2^19 PRPs by doubling up to half the buffer, so the
+    // one copy that nothing overlaps (the first) is short and every later
+    // copy hides behind the test of the chunk before it.
+    const u64 maxc = std::min<u64>(c->cap / 2, 0xffffffffull);
+    // the previous call's copy of the count table may still read h_chunk
     WW_CU(cudaStreamSynchronize(c->stream));
-    for (u64 i = 0; i < nchunks; ++i) {
-        c->h_chunk[2 * i] = (u32)std::min<u64>(chunk, n - i * chunk);
-        c->h_chunk[2 * i + 1] = 0;
+    u64 nchunks = 0;
+    for (u64 done = 0, len = std::min<u64>(1ull << 19, maxc); done < n; len = std::min<u64>(2 * len, maxc)) {
+        if (nchunks == kHostChunksMax)
+            return set_err("list of %llu PRPs needs a larger PRP buffer (capacity %llu)", (unsigned long long)n,
+                           (unsigned long long)c->cap), WW_ERR_ARG;
+        const u64 take = std::min<u64>(len, n - done);
+        c->h_chunk[2 * nchunks] = (u32)take;
+        c->h_chunk[2 * nchunks + 1] = 0;
+        ++nchunks;
+        done += take;
     }
     WW_CU(cudaMemcpyAsync(c->d_chunk, c->h_chunk, 2 * nchunks * sizeof(u32), cudaMemcpyHostToDevice, c->stream));
     WW_CU(cudaMemsetAsync(c->d_cursor + 5, 0, nchunks * sizeof(u64), c->stream));
@@ -521,12 +523,13 @@ int ww_test_prps_host(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
     WW_CU(cudaEventRecord(c->consumed[0], c->stream));
     WW_CU(cudaEventRecord(c->consumed[1], c->stream));
     HitOut h{c->hprime, c->hrem, c->hquot, c->hres, &c->dc->resultcount, c->hcap, &c->dc->overflow};
+    u64 offset = 0;
     for (u64 i = 0; i < nchunks; ++i) {
         const int half = (int)(i & 1);
-        u64 *dst = c->prime + (u64)half * chunk;
+        u64 *dst = c->prime + (u64)half * maxc;
         const u64 len = c->h_chunk[2 * i];
         WW_CU(cudaStreamWaitEvent(c->copy_stream, c->consumed[half], 0));
-        WW_CU(cudaMemcpyAsync(dst, host_primes + i * chunk, len * 8, cudaMemcpyHostToDevice, c->copy_stream));
+        WW_CU(cudaMemcpyAsync(dst, host_primes + offset, len * 8, cudaMemcpyHostToDevice, c->copy_stream));
         WW_CU(cudaEventRecord(c->copied[half], c->copy_stream));
         WW_CU(cudaStreamWaitEvent(c->stream, c->copied[half], 0));
         k_test_prps<<<test_grid(), kTestThreads, 0, c->stream>>>(c->d_chunk + 2 * i, dst, nullptr, h,
@@ -534,6 +537,7 @@ int ww_test_prps_host(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
                                                                  len, c->d_cursor + 5 + i);
         WW_CHECK_LAUNCH();
         WW_CU(cudaEventRecord(c->consumed[half], c->stream));
+        offset += len;
     }
     return WW_OK;
 }
