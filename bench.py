@@ -51,6 +51,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--range-width", type=float, default=float(1 << 34),
                     help="width of the plain-path range leg starting at 2^64-2^35 (0: skip)")
+    ap.add_argument("--batch-config", default="",
+                    help="force the batched configuration SEG_WORDS/THREADS/PPT instead of the autotuner's choice")
     ap.add_argument("--batch-units", type=int, default=128,
                     help="units of the uneven mix for the batched-vs-plain line (0: skip)")
     ap.add_argument("--serve-seconds", type=float, default=10.0,
@@ -253,14 +255,19 @@ def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30) -> dict:
     return out
 
 
-def compare_batched_plain(ww, local: int, units: list, workload: str, tune_units: int = 32) -> dict:
+def compare_batched_plain(ww, local: int, units: list, workload: str, tune_units: int = 32,
+                          force_cfg: tuple | None = None) -> dict:
     """Plain = one range per launch sequence (clear, sieve, test, read)
     through the context API; batched = one persistent CUDA-graph launch over
     the tile queue after the autotuner picked the configuration.  Per-unit
     checksums and PRP counts must agree."""
     ctx = ww.Context(local, max_prps=ww.prp_count_bound(0, 1 << 30), max_hits=15000)
     b = ww.Batch(ctx)
-    cfg, _ = b.tune(units[:tune_units])
+    if force_cfg:
+        b.set_config(*force_cfg)
+        cfg = b.config()
+    else:
+        cfg, _ = b.tune(units[:tune_units])
     b.run(units)  # warm
     ctx.marker(0)
     res = b.run(units)
@@ -315,17 +322,17 @@ def compare_batched_plain(ww, local: int, units: list, workload: str, tune_units
                              "primes_per_thread": cfg[2]}}
 
 
-def run_batched_vs_plain(ww, local: int, n_units: int) -> dict:
+def run_batched_vs_plain(ww, local: int, n_units: int, force_cfg: tuple | None = None) -> dict:
     """The seed-11 uneven mix (4096 units, widths log-uniform in [1e6, 1e10],
     starts uniform in [1e15, 2^64-1e10], multiples of 30): its first n_units
     units, and separately its first 2*n_units units narrower than 1e8 (where
     one launch sequence per range leaves most of the GPU idle)."""
     mix = ww.uneven_units(11, 4096)
     out = compare_batched_plain(ww, local, mix[:n_units],
-                                f"first {n_units} units of the seed-11 uneven mix (4096 units)")
+                                f"first {n_units} units of the seed-11 uneven mix (4096 units)", force_cfg=force_cfg)
     narrow = [u for u in mix if u[1] - u[0] < 10**8][: 2 * n_units]
     out["narrow_units"] = compare_batched_plain(
-        ww, local, narrow, f"first {len(narrow)} units of the same mix narrower than 1e8")
+        ww, local, narrow, f"first {len(narrow)} units of the same mix narrower than 1e8", force_cfg=force_cfg)
     return out
 
 
@@ -530,7 +537,8 @@ def main():
     if args.range_width:
         extra["range_pipeline"] = run_range_pipeline(ww, local, int(args.range_width))
     if args.batch_units:
-        extra["batched_vs_plain"] = run_batched_vs_plain(ww, local, args.batch_units)
+        force = tuple(int(x) for x in args.batch_config.split("/")) if args.batch_config else None
+        extra["batched_vs_plain"] = run_batched_vs_plain(ww, local, args.batch_units, force)
     if args.serve_seconds:
         extra["serving"] = run_serving(ww, local, args.serve_seconds)
 
