@@ -56,3 +56,17 @@ def test_two_rank_split_sums_to_reference(ww, ctx):
         total_n += sum(u["prp_count"] for u in got)
     assert total_n == LONG["prp_count"]
     assert "%016X" % (total_c % 2**64) == LONG["checksum"]
+
+
+@pytest.mark.parametrize("case", [1, 2, 3])
+def test_shard_entry_writes_reference_results(tests_txt, tmp_path, case):
+    """shard.py's entry point (what torchrun starts on each GPU) on the
+    reference's tests.txt vectors: the results file it writes -- prime hits,
+    then the hex checksum -- equals the reference's, and search_range on one
+    rank reports the same checksum."""
+    import shard
+
+    c = tests_txt[case]
+    out = tmp_path / "results.txt"
+    assert shard.main([c["start"], c["end"], "--results", str(out)]) == 0
+    assert out.read_text().splitlines() == c["hits"] + [c["checksum"]]

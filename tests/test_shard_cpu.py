@@ -35,11 +35,14 @@ def _rank_main(rank, world, port, lo, hi, out):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
-    a, b = shard.split_range(lo, hi, world, rank)
-    summ, _, hits = Oracle().scan_range(a, b, nthreads=2, hit_cap=100000)
-    cks, cnt = shard.reduce_sums(summ["checksum"], summ["prp_count"])
-    allhits = shard.gather_hits(hits)
-    out[rank] = (cks, cnt, allhits, (a, b))
+    oracle = Oracle()
+
+    def cpu_searcher(a, b):  # the oracle stands in for this rank's GPU
+        summ, _, hits = oracle.scan_range(a, b, nthreads=2, hit_cap=100000)
+        return summ["checksum"], summ["prp_count"], hits
+
+    r = shard.search_range(lo, hi, cpu_searcher)
+    out[rank] = (r["checksum"], r["prp_count"], r["hits"], r["piece"])
     dist.barrier()
     dist.destroy_process_group()
 
