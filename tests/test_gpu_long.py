@@ -62,11 +62,13 @@ def test_two_rank_split_sums_to_reference(ww, ctx):
 def test_shard_entry_writes_reference_results(tests_txt, tmp_path, case):
     """shard.py's entry point (what torchrun starts on each GPU) on the
     reference's tests.txt vectors: the results file it writes -- prime hits,
-    then the hex checksum -- equals the reference's, and search_range on one
-    rank reports the same checksum."""
+    then the hex checksum -- equals the reference's."""
     import shard
 
     c = tests_txt[case]
     out = tmp_path / "results.txt"
     assert shard.main([c["start"], c["end"], "--results", str(out)]) == 0
-    assert out.read_text().splitlines() == c["hits"] + [c["checksum"]]
+    lines = out.read_text().splitlines()
+    assert lines[-1] == c["checksum"]
+    if c["hits"]:  # the [1, 6e10) vector lists its checksum only, not its small special instances
+        assert lines[:-1] == c["hits"]
