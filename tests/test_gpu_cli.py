@@ -76,3 +76,18 @@ def test_finished_workunit_exits_early(tmp_path):
 def test_bad_range_is_an_error(tmp_path):
     r = run(["2e6", "1e6"], tmp_path)
     assert r.returncode != 0 and "END must be > START" in r.stdout
+
+
+def test_debug_prints_kernel_profile_and_counters(tests_txt, tmp_path):
+    """-debug (main.cpp:1632-1661, 932-939): the per-kernel time shares of one
+    segment and the checkpoint counters; the search result is unchanged."""
+    c = tests_txt[2]
+    r = run([c["start"], c["end"], "-debug"], tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = r.stdout
+    assert "Profiling kernels..." in out and "Percent of time spent in each kernel:" in out
+    for name in ("Prime Generator:", "Wieferich Test:", "WallSunSun Test:"):
+        assert name in out
+    assert "PRPs tested since last checkpoint:" in out
+    lines = (tmp_path / "results-WW.txt").read_text().splitlines()
+    assert lines == c["hits"] + [c["checksum"]]

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/wwcuda.h"
+#include "ww_trace.hpp"
 #include "ww_batch.cuh"
 
 using namespace ww;
@@ -300,6 +301,7 @@ int ww_batch_reserve_hits(ww_ctx *ctx, uint32_t max_hits) {
 }
 
 int ww_batch_submit(ww_ctx *ctx, const ww_unit *units, uint32_t n) {
+    ww::TraceRange trace("ww_batch_submit");
     if (!ctx || (!units && n)) return set_err("null argument"), WW_ERR_ARG;
     BatchState *&bs = ctx_batch(ctx);
     if (!bs) bs = new (std::nothrow) BatchState;
@@ -312,6 +314,7 @@ int ww_batch_submit(ww_ctx *ctx, const ww_unit *units, uint32_t n) {
 }
 
 int ww_batch_collect(ww_ctx *ctx, ww_unit_result *out, uint32_t n, uint32_t *hit_count) {
+    ww::TraceRange trace("ww_batch_collect");
     if (!ctx || (!out && n)) return set_err("null argument"), WW_ERR_ARG;
     BatchState *bs = ctx_batch(ctx);
     if (!bs || n > bs->n_units) return set_err("no batch of %u units submitted", n), WW_ERR_STATE;
@@ -368,6 +371,7 @@ int ww_batch_hits(ww_ctx *ctx, ww_hit *out, uint32_t *unit_of_hit, uint32_t cap,
 // Time every compiled configuration on the sample (after one warm-up run
 // each) and keep the fastest in the context.
 int ww_batch_tune(ww_ctx *ctx, const ww_unit *sample, uint32_t n, ww_batch_cfg *best, float *best_ms) {
+    ww::TraceRange trace("ww_batch_tune");
     if (!ctx || !sample || n == 0) return set_err("bad argument"), WW_ERR_ARG;
     BatchState *&bs = ctx_batch(ctx);
     if (!bs) bs = new (std::nothrow) BatchState;
@@ -603,6 +607,7 @@ int ww_server_status(ww_ctx *ctx, uint32_t *queued, uint32_t *active, uint64_t *
 }
 
 int ww_server_step(ww_ctx *ctx, ww_request_result *done, uint32_t cap, uint32_t *ndone) {
+    ww::TraceRange trace("ww_server_step");
     ServerState *sv = ctx ? ctx_server(ctx) : nullptr;
     if (!sv) return set_err("server not open"), WW_ERR_STATE;
     if (!ndone || (!done && cap)) return set_err("null argument"), WW_ERR_ARG;

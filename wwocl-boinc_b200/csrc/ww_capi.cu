@@ -11,6 +11,7 @@
 #include <thread>
 
 #include "../../include/wwcuda.h"
+#include "ww_trace.hpp"
 #include "ww_kernels.cuh"
 
 using namespace ww;
@@ -430,12 +431,14 @@ int ww_clear_segment(ww_ctx *c) {
     } while (0)
 
 int ww_sieve_prp(ww_ctx *c, uint64_t kernel_start, uint64_t stop, int32_t wheel_idx) {
+    ww::TraceRange trace("ww_sieve_prp");
     WW_NEED_BUFFERS(c);
     return launch_sieve(kernel_start, stop, wheel_idx, (uint64_t *)c->prime, (uint64_t *)c->inv, c->dc->primecount,
                         c->cap, &c->dc->overflow, c->stream, c->d_cursor + 1);
 }
 
 int ww_wieferich(ww_ctx *c) {
+    ww::TraceRange trace("ww_wieferich");
     WW_NEED_BUFFERS(c);
     WW_CU(cudaMemsetAsync(c->d_cursor + 2, 0, sizeof(u64), c->stream));
     HitOut h{c->hprime, c->hrem, c->hquot, c->hres, &c->dc->resultcount, c->hcap, &c->dc->overflow};
@@ -447,6 +450,7 @@ int ww_wieferich(ww_ctx *c) {
 }
 
 int ww_wallsunsun(ww_ctx *c) {
+    ww::TraceRange trace("ww_wallsunsun");
     WW_NEED_BUFFERS(c);
     WW_CU(cudaMemsetAsync(c->d_cursor + 3, 0, sizeof(u64), c->stream));
     HitOut h{c->hprime, c->hrem, c->hquot, c->hres, &c->dc->resultcount, c->hcap, &c->dc->overflow};
@@ -458,6 +462,7 @@ int ww_wallsunsun(ww_ctx *c) {
 }
 
 int ww_test_prps(ww_ctx *c) {
+    ww::TraceRange trace("ww_test_prps");
     WW_NEED_BUFFERS(c);
     WW_CU(cudaMemsetAsync(c->d_cursor, 0, sizeof(u64), c->stream));
     HitOut h{c->hprime, c->hrem, c->hquot, c->hres, &c->dc->resultcount, c->hcap, &c->dc->overflow};
@@ -486,6 +491,7 @@ int ww_load_prps(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
 }
 
 int ww_test_prps_host(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
+    ww::TraceRange trace("ww_test_prps_host");
     WW_NEED_BUFFERS(c);
     if (!host_primes && n) return set_err("null list"), WW_ERR_ARG;
     if (n == 0) return WW_OK;
@@ -543,6 +549,7 @@ int ww_test_prps_host(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
 }
 
 int ww_count_prps(ww_ctx *c, uint64_t lo, uint64_t hi, uint64_t *count) {
+    ww::TraceRange trace("ww_count_prps");
     if (!c || !count) return set_err("null argument"), WW_ERR_ARG;
     if (lo < 127 || hi < lo) return set_err("bad range [%llu, %llu)", (unsigned long long)lo,
                                             (unsigned long long)hi), WW_ERR_ARG;

@@ -25,6 +25,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../host/wwhost.hpp"
 #include "wwcuda.h"
 
@@ -132,6 +134,37 @@ void enqueue_segment(ww_ctx *ctx, uint64_t start, uint64_t stop, bool separate) 
     } else {
         must(ww_test_prps(ctx), "test_prps");
     }
+}
+
+// -debug's kernel profile (main.cpp:1632-1661): one segment's sieve,
+// Wieferich and WallSunSun kernels timed with events, as shares of the sum.
+void profile_kernels(ww_ctx *ctx, uint64_t start, uint64_t stop) {
+    printf("Profiling kernels...\n");
+    uint64_t ks = start;
+    int32_t idx = 0;
+    if (ww_find_wheel_offset(&ks, &idx) != WW_OK || ks >= stop) return;
+    must(ww_clear_results(ctx), "clearresult");
+    must(ww_clear_segment(ctx), "clearn");
+    must(ww_marker(ctx, 1), "marker");
+    must(ww_sieve_prp(ctx, ks, stop, idx), "getsegprimes");
+    must(ww_marker(ctx, 2), "marker");
+    must(ww_wieferich(ctx), "wieferich");
+    must(ww_marker(ctx, 3), "marker");
+    must(ww_wallsunsun(ctx), "wallsunsun");
+    must(ww_marker(ctx, 4), "marker");
+    must(ww_sync(ctx, 600000), "sync");
+    float prime_ms = 0, wie_ms = 0, wall_ms = 0;
+    must(ww_marker_elapsed(ctx, 1, 2, &prime_ms), "elapsed");
+    must(ww_marker_elapsed(ctx, 2, 3, &wie_ms), "elapsed");
+    must(ww_marker_elapsed(ctx, 3, 4, &wall_ms), "elapsed");
+    const double total = (double)prime_ms + wie_ms + wall_ms;
+    const int prime_pct = (int)(prime_ms / total * 100.0), wie_pct = (int)(wie_ms / total * 100.0),
+              wall_pct = (int)(wall_ms / total * 100.0);
+    printf("Percent of time spent in each kernel:\n");
+    printf("\tPrime Generator:\t%d %%\t(%0.1f ms)\n\tWieferich Test:\t\t%d %%\t(%0.1f ms)\n"
+           "\tWallSunSun Test:\t%d %%\t(%0.1f ms)\n",
+           prime_pct, prime_ms, wie_pct, wie_ms, wall_pct, wall_ms);
+    must(ww_clear_results(ctx), "clearresult");
 }
 
 // checkPRPS (main.cpp:451-523): the GPU PRP list minus base-2 pseudoprimes
@@ -331,6 +364,11 @@ int main(int argc, char **argv) {
     must(ww_reserve(ctx, mem_size, kNumResults), "reserve");
     if (o.debug) printf("segment width %" PRIu64 ", PRP buffer %" PRIu64 "\n", calc_range, mem_size);
 
+    if (o.debug) {
+        uint64_t k_stop = st.current + calc_range;
+        if (k_stop > top || k_stop < st.current) k_stop = top;
+        profile_kernels(ctx, st.current, k_stop);
+    }
     self_test(ctx, st.current, top, calc_range, mem_size, o.debug, o.separate);
 
     fprintf(stderr, "Starting search...\n");
@@ -359,7 +397,9 @@ int main(int argc, char **argv) {
             if (boinc::is_standalone()) printf("Tests done: %.4f%%\n", fd * 100.0);
             last_progress = t;
         }
+        nvtxRangePushA("segment");
         enqueue_segment(ctx, start, stop, o.separate);
+        nvtxRangePop();
         if (iter == 0) must(ww_marker(ctx, 0), "marker");
         ++iter;
         since_ckpt += stop - start;
@@ -373,6 +413,7 @@ int main(int argc, char **argv) {
         if (ckpt_secs > 60.0 || stop == top || by_count) {  // main.cpp:1743-1792
             must(ww_sync(ctx, 0), "sync");
             iter = 0;
+            nvtxRangePushA("checkpoint");
             boinc::begin_critical_section();
             get_results(ctx, o, now_s() - last_ckpt, st, mem_size);
             if (stop == top) {
@@ -390,6 +431,7 @@ int main(int argc, char **argv) {
             if (boinc::is_standalone()) printf("Checkpoint, current: %" PRIu64 "\n", stop);
             boinc::checkpoint_completed();
             boinc::end_critical_section();
+            nvtxRangePop();
             last_ckpt = now_s();
             since_ckpt = 0;
             must(ww_clear_results(ctx), "clearresult");
