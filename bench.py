@@ -351,7 +351,7 @@ def run_serving(ww, local: int, seconds: float, rate: float = 200.0, seed: int =
     starts = rng.integers(10**12, 2**64 - 10**9, len(arrivals), dtype=np.uint64)
     reqs = [(i, int(s), int(s) + int(w)) for i, (s, w) in enumerate(zip(starts, widths))]
     ctx = ww.Context(local, max_prps=1 << 20, max_hits=15000)
-    srv = ww.Server(ctx, prp_pool_bytes=24 << 30, max_active=256, epoch_tiles=1024, store_prps=True)
+    srv = ww.Server(ctx, prp_pool_bytes=24 << 30, max_active=256, epoch_tiles=0, store_prps=True)  # one wave of resident CTAs per step
     srv.submit([(10**9, 10**12, 10**12 + 10**6)])  # warm-up request
     srv.drain()
     done = {}

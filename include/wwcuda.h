@@ -280,7 +280,8 @@ typedef struct {
     uint64_t prp_pool_bytes; /* device memory for per-request PRP buffers */
     uint32_t max_active;     /* device slots */
     uint32_t epoch_tiles;    /* tiles one step launches (rounded to whole
-                                waves of resident CTAs when above one wave) */
+                                waves of resident CTAs when above one wave;
+                                0: one wave) */
     uint32_t max_hits;       /* hit records per step */
     uint32_t store_prps;     /* 1: keep each request's PRP list on the device */
 } ww_server_cfg;
@@ -363,10 +364,10 @@ int ww_selftest_m2(int op, uint64_t p, const uint64_t *xy, uint64_t n, uint64_t 
 /* The kernels' PRP-test candidates of [lo, hi) computed on the host
  * (small primes 3..113, then the deep sieve, which leaves unmarked every
  * multiple r*k with k = 1 (mod ord_r(2)): r itself and every possible
- * base-2 pseudoprime with the factor r), sorted; *rescued = the number of
+ * base-2 pseudoprime with the factor r), sorted; *spared = the number of
  * deep-prime multiples left unmarked that way. */
 int ww_selftest_candidates(uint64_t lo, uint64_t hi, uint64_t *out, uint64_t cap, uint64_t *n,
-                           uint64_t *rescued);
+                           uint64_t *spared);
 
 /* ---------------------------------------------------------------------------
  * 4. Measurement utilities (no reference counterpart).

@@ -165,7 +165,7 @@ def test_deep_sieve_keeps_every_prp(ww, oracle, lo, hi):
     """The deep sieve (primes to 2^20), which spares every multiple r*k with
     k = 1 (mod ord_r(2)), keeps every PRP of the reference's definition, and
     only numbers with no factor <= 113 reach the PRP test."""
-    cand, rescued = ww.selftest_candidates(lo, hi)
+    cand, spared = ww.selftest_candidates(lo, hi)
     summ, prps, _ = oracle.scan_range(lo, hi, want_prps=True, prp_cap=(hi - lo) // 2 + 8)
     assert np.unique(cand).size == cand.size, "a candidate would be tested twice"
     assert np.all(np.isin(prps, cand)), "a PRP was sieved out"
@@ -185,8 +185,8 @@ def test_deep_sieve_spares_pseudoprimes_with_deep_factors(ww, oracle):
     # whose factors are deep-sieve primes: only the cofactor rule keeps them
     for n in (49141, 88357, 104653):
         assert oracle.is_prp(n) and not oracle.is_prime(n)
-        cand, rescued = ww.selftest_candidates(n - 2000, n + 2000)
-        assert cand.tolist().count(n) == 1 and rescued >= 1
+        cand, spared = ww.selftest_candidates(n - 2000, n + 2000)
+        assert cand.tolist().count(n) == 1 and spared >= 1
     # 49141 is spared by both of its factors; it must reach the PRP test once
-    cand, rescued = ww.selftest_candidates(49141 - 10, 49141 + 10)
-    assert rescued >= 2 and cand.tolist().count(49141) == 1
+    cand, spared = ww.selftest_candidates(49141 - 10, 49141 + 10)
+    assert spared >= 2 and cand.tolist().count(49141) == 1

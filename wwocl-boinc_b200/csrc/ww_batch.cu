@@ -71,7 +71,9 @@ const CfgEntry *find_cfg(const ww_batch_cfg &c) {
     return nullptr;
 }
 
-ww_batch_cfg default_cfg() { return ww_batch_cfg{8192, 256, 1, 0}; }
+// the configuration the autotuner picks on the uneven mix, and the one that
+// gave the request server its lowest latencies
+ww_batch_cfg default_cfg() { return ww_batch_cfg{16384, 512, 1, 0}; }
 
 }  // namespace
 
@@ -526,7 +528,7 @@ double mono_s() {
 extern "C" {
 
 int ww_server_open(ww_ctx *ctx, const ww_server_cfg *cfg) {
-    if (!ctx || !cfg || cfg->max_active == 0 || cfg->epoch_tiles == 0 || cfg->max_hits == 0)
+    if (!ctx || !cfg || cfg->max_active == 0 || cfg->max_hits == 0)
         return set_err("bad server configuration"), WW_ERR_ARG;
     WW_CU(cudaSetDevice(ctx_device(ctx)));
     ServerState *&sv = ctx_server(ctx);
@@ -670,7 +672,8 @@ int ww_server_step(ww_ctx *ctx, ww_request_result *done, uint32_t cap, uint32_t 
     // whole waves of the resident CTAs: a partial last wave would leave most
     // SMs idle while its few tiles finish
     const u32 g = (u32)s.grid;
-    a.budget = s.cfg.epoch_tiles < g ? s.cfg.epoch_tiles : std::max(1u, (s.cfg.epoch_tiles + g / 2) / g) * g;
+    if (s.cfg.epoch_tiles == 0) a.budget = g;  // one wave
+    else a.budget = s.cfg.epoch_tiles < g ? s.cfg.epoch_tiles : std::max(1u, (s.cfg.epoch_tiles + g / 2) / g) * g;
     a.hit_p = s.d_hit_p;
     a.hit_result = s.d_hit_res;
     a.hit_rem = s.d_hit_rem;

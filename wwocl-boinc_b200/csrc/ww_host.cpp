@@ -275,7 +275,7 @@ const DeepRow kDeepHost[WW_DEEP_COUNT] = {WW_DEEP_ROWS(WW_DEEP_ROWH)};
 }  // namespace
 
 extern "C" int ww_selftest_candidates(uint64_t lo, uint64_t hi, uint64_t *out, uint64_t cap, uint64_t *n,
-                                      uint64_t *rescued) {
+                                      uint64_t *spared_out) {
     if (!n || (!out && cap) || hi <= lo || lo < 127 || hi - lo > (1ull << 32)) return WW_ERR_ARG;
     const u64 b0 = lo & ~1ull, first = b0 + 1;
     const u64 nvalid = (hi - b0) / 2;
@@ -301,7 +301,7 @@ extern "C" int ww_selftest_candidates(uint64_t lo, uint64_t hi, uint64_t *out, u
     for (u64 j = 0; j < nvalid; ++j)
         if (!((bitmap[j >> 5] >> (j & 31)) & 1u)) cand.push_back(first + 2 * j);
     *n = cand.size();
-    if (rescued) *rescued = spared;
+    if (spared_out) *spared_out = spared;
     for (u64 i = 0; i < cap && i < cand.size(); ++i) out[i] = cand[i];
     return WW_OK;
 }

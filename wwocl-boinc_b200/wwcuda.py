@@ -487,7 +487,7 @@ class Server:
     """Continuous-batching request server on a Context."""
 
     def __init__(self, ctx: Context, prp_pool_bytes: int = 8 << 30, max_active: int = 64,
-                 epoch_tiles: int = 2048, max_hits: int = 1 << 15, store_prps: bool = True):
+                 epoch_tiles: int = 0, max_hits: int = 1 << 15, store_prps: bool = True):
         self.ctx = ctx
         cfg = ServerCfg(prp_pool_bytes, max_active, epoch_tiles, max_hits, 1 if store_prps else 0)
         check(_L.ww_server_open(ctx.h, C.byref(cfg)), "ww_server_open")
