@@ -322,6 +322,44 @@ def compare_batched_plain(ww, local: int, units: list, workload: str, tune_units
                              "primes_per_thread": cfg[2]}}
 
 
+def compare_batched_per_run(ww, local: int, units: list, workload: str) -> dict:
+    """The reference's deployment: one program run per range (a BOINC work
+    unit), each with its own device set-up, work-size profiling and start-up
+    self-test (main.cpp:959-1107, 590-738), here bin/wwocl started once per
+    range; against one batched launch over the same ranges.  Each run's
+    final checksum (results file) must equal the batched per-range one."""
+    import tempfile
+
+    exe = ROOT / "wwocl-boinc_b200" / "bin" / "wwocl"
+    if not exe.exists():
+        return {"workload": workload, "unavailable": "bin/wwocl not built"}
+    ctx = ww.Context(local, max_prps=1 << 20, max_hits=15000)
+    b = ww.Batch(ctx)
+    b.run(units)  # warm
+    ctx.marker(0)
+    res = b.run(units)
+    ctx.marker(1)
+    ctx.sync()
+    batch_ms = ctx.elapsed_ms(0, 1)
+    ctx.close()
+    equal = True
+    t0 = time.perf_counter()
+    for (a, z), r in zip(units, res):
+        with tempfile.TemporaryDirectory() as d:
+            p = subprocess.run([str(exe), str(a), str(z), "-device", str(local)], cwd=d, capture_output=True,
+                               text=True, timeout=600)
+            lines = (Path(d) / "results-WW.txt").read_text().splitlines() if p.returncode == 0 else []
+        equal &= bool(lines) and lines[-1] == "%016X" % r["checksum"]
+    per_run_s = time.perf_counter() - t0
+    prps = sum(r["prp_count"] for r in res)
+    return {"workload": workload, "units": len(units), "prps": prps,
+            "batched_primes_per_s": prps / (batch_ms * 1e-3), "per_run_primes_per_s": prps / per_run_s,
+            "speedup_batched_vs_per_run": per_run_s / (batch_ms * 1e-3),
+            "per_run_definition": "bin/wwocl START END once per range: device set-up, work-size profiling, "
+                                  "start-up self-test, the range, results file",
+            "checksums_equal": bool(equal)}
+
+
 def run_batched_vs_plain(ww, local: int, n_units: int, force_cfg: tuple | None = None) -> dict:
     """The seed-11 uneven mix (4096 units, widths log-uniform in [1e6, 1e10],
     starts uniform in [1e15, 2^64-1e10], multiples of 30): its first n_units
@@ -333,6 +371,9 @@ def run_batched_vs_plain(ww, local: int, n_units: int, force_cfg: tuple | None =
     narrow = [u for u in mix if u[1] - u[0] < 10**8][: 2 * n_units]
     out["narrow_units"] = compare_batched_plain(
         ww, local, narrow, f"first {len(narrow)} units of the same mix narrower than 1e8", force_cfg=force_cfg)
+    k = max(1, n_units // 16)
+    out["per_run"] = compare_batched_per_run(ww, local, mix[:k],
+                                             f"first {k} units of the same mix, one program run per range")
     return out
 
 
