@@ -575,6 +575,8 @@ def main():
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 
     extra = {}
+    if world > 1:  # the single-GPU legs below are measured at N = 1; a scaling run keeps its GPUs short
+        args.range_width = args.batch_units = args.serve_seconds = 0
     if args.range_width:
         extra["range_pipeline"] = run_range_pipeline(ww, local, int(args.range_width))
     if args.batch_units:
