@@ -101,9 +101,34 @@ WW_HD u64 mont_mul(u64 a, u64 b, u64 n, u64 q) {
     return redc(lo, hi, n, q);
 }
 
+// For odd n in [2^32, 2^63): q = floor(2^64 / n) and 2^64 - q n.  On the
+// device the quotient comes from a double-precision estimate (off by at most
+// one) corrected exactly, instead of the 64-bit division subroutine, which
+// would also split the lanes of a warp.
+WW_HD u64 div_r64(u64 n, u64 &q_out) {
+#if defined(__CUDA_ARCH__)
+    u64 q = (u64)(18446744073709551616.0 / (double)n);
+    if (mul_hi(q, n) != 0) --q;  // q n >= 2^64 (never equal: n is odd and > 1)
+    u64 rem = 0 - q * n;         // 2^64 - q n, in [0, 2n)
+    if (rem >= n) {
+        rem -= n;
+        ++q;
+    }
+    q_out = q;
+    return rem;
+#else
+    q_out = (0 - n) / n + 1;
+    return (0 - n) % n;
+#endif
+}
+
 // 2^64 mod n for odd n > 1.
 WW_HD u64 r_mod(u64 n) {
     if (n >> 63) return 0 - n;  // 2^64 - n < n
+    if (n >> 32) {
+        u64 q;
+        return div_r64(n, q);
+    }
     return (0 - n) % n;
 }
 
@@ -283,9 +308,10 @@ WW_HD D2 m2_one(u64 p) {
         r.d1 = 1;
         return r;
     }
-    const u64 mp = 0 - p;
-    r.d0 = mp % p;
-    r.d1 = mp / p + 1;
+    // 2^32 <= p < 2^63: 2^64 = q p + rem with q < p
+    u64 q;
+    r.d0 = div_r64(p, q);
+    r.d1 = q;
     return r;
 }
 
