@@ -135,8 +135,9 @@ WW_HD u64 r_mod(u64 n) {
 // Base-2 strong probable-prime test (prime.h:65-114, getsegprimes.cl:118-164)
 // written as one uniform loop over the bits of n-1 so that a warp's lanes
 // stay converged whatever the 2-adic valuation t of n-1 is: the trailing t
-// zero bits square without doubling, and the checks fire at bit t (a^d = +-1)
-// and below it (a^(d 2^s) = -1).  Returns the result and n^-1 mod 2^64.
+// zero bits square without doubling; the loop keeps a^d (the value at bit t)
+// and whether a^(d 2^s) = -1 below it, and the checks run once at the end.
+// Returns the result and n^-1 mod 2^64.
 WW_HD bool sprp2(u64 n, u64 &q_out) {
     const u64 q = inv64(n);
     q_out = q;
@@ -151,14 +152,16 @@ WW_HD bool sprp2(u64 n, u64 &q_out) {
     const int top = 63 - __builtin_clzll(nm1);
 #endif
     u64 a = add_mod(one, one, n);  // 2 for the leading bit
-    bool ok = false;
+    u64 at_t = 0;                  // 2^d, the value at bit t
+    bool m1 = false;               // 2^(d 2^s) = -1 for some 0 < s < t
     for (int i = top - 1; i >= 1; --i) {
         a = mont_mul(a, a, n, q);
         const u64 d = add_mod(a, a, n);
         a = ((nm1 >> i) & 1) ? d : a;
-        ok |= (i == t) & ((a == one) | (a == mone));
-        ok |= (i < t) & (a == mone);
+        at_t = (i == t) ? a : at_t;
+        m1 |= (i < t) & (a == mone);
     }
+    bool ok = (at_t == one) | (at_t == mone) | m1;
     if (t == 0) ok = false;  // even n is never a candidate
     // t == top (n-1 a power of two) never happens for the odd n >= 127 tested
     return ok;
