@@ -197,7 +197,7 @@ def run_reference(args):
     return 0
 
 
-def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30) -> dict:
+def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30, chain_peak: float | None = None) -> dict:
     """The plain one-range path over [2^64-2^35, 2^64-2^35+width): per 2^30
     numbers (the checkpoint cadence) clear, sieve + SPRP, both tests, sync and
     read the counters back, as the reference program's loop does.  With the
@@ -247,6 +247,24 @@ def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30) -> dict:
                             "sieve_numbers_per_s": min(width, ckpt) / (sieve_ms * 1e-3),
                             "test_primes_per_s": seg_prps / (test_ms * 1e-3)},
            "checksum": "%016X" % cks, "results": res}
+    if chain_peak:
+        # end to end over sieve + tests, in the same 32-bit multiply units as
+        # the test kernel's roofline (k = 64 here): the SPRP of a candidate is
+        # 20(k-1); the reference's sieve hands ~5.3 candidates per PRP to it,
+        # the deep sieve here ~1.8 (0.5615 / ln 2^20 per integer over the PRP
+        # density 1 / ln 2^64)
+        k = 64
+        sprp = 20.0 * (k - 1)
+        ref_ops = 40.0 * (k - 3) + 128.0 * (k - 1) + 5.3 * sprp
+        cand = (0.5615 / np.log(2.0**20)) * np.log(2.0**64)
+        run_ops = 40.0 * (k - 2) + 80.0 * (k - 1) + 48.0 + cand * sprp
+        rate = out["primes_per_s"]
+        out["roofline_end_to_end"] = {
+            "peak_tops": chain_peak / 1e12,
+            "reference_ops_per_prime": ref_ops, "frac_reference_ops": rate * ref_ops / chain_peak,
+            "executed_ops_per_prime": run_ops, "frac_executed_ops": rate * run_ops / chain_peak,
+            "note": "reference ops count the reference algorithm's work (more SPRP candidates, a longer "
+                    "Lucas ladder); above 1.0 means less work than the reference needs, not above peak"}
     golden = ROOT / "tests" / "golden" / "ref_long.json"
     if golden.exists():
         g = json.loads(golden.read_text())["config3"]
@@ -578,7 +596,7 @@ def main():
     if world > 1:  # the single-GPU legs below are measured at N = 1; a scaling run keeps its GPUs short
         args.range_width = args.batch_units = args.serve_seconds = 0
     if args.range_width:
-        extra["range_pipeline"] = run_range_pipeline(ww, local, int(args.range_width))
+        extra["range_pipeline"] = run_range_pipeline(ww, local, int(args.range_width), chain_peak=chain_peak)
     if args.batch_units:
         force = tuple(int(x) for x in args.batch_config.split("/")) if args.batch_config else None
         extra["batched_vs_plain"] = run_batched_vs_plain(ww, local, args.batch_units, force)
