@@ -8,7 +8,7 @@
 // shared counter (so the warps of a CTA finish a tile together), compact
 // the survivors into a warp queue, run the base-2 strong PRP test 32 at a
 // time, and push the PRPs into a second warp queue that feeds the
-// Wieferich + Wall-Sun-Sun ladder 32 (or 64 with two primes per thread) at
+// Wieferich and Wall-Sun-Sun tests 32 (or 64 with two primes per thread) at
 // a time.  Checksums and PRP counts go to the tile's unit with one atomic
 // per warp per batch; the sums are order-free, so every unit's checksum is
 // bit-identical to a run of that unit alone.

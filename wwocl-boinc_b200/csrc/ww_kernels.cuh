@@ -1,16 +1,20 @@
 // ww_kernels.cuh -- kernels of the WWocl search path on sm_100a.
 //
-//   k_sieve_prp   getsegprimes (getsegprimes.cl:228-301): one CTA per segment
-//                 of 2*kSegOdd integers.  The odd numbers of the segment form a
+//   k_sieve_prp   getsegprimes (getsegprimes.cl:228-301): a CTA sieves one
+//                 segment of 2*kSegOdd integers at a time (taken from a cursor,
+//                 or by grid stride).  The odd numbers of the segment form a
 //                 shared-memory bitmap; each thread ORs the composite patterns
 //                 of 3..113 into its words (the reference's 27 constant tables,
 //                 getsegprimes.cl:169-225, become per-prime bit offsets kept
-//                 incrementally), then each warp compacts the survivors with
+//                 incrementally), the deep sieve marks the multiples of the
+//                 primes up to 2^WW_DEEP_BITS that cannot be pseudoprimes
+//                 (ww_deep.cuh), then each warp compacts the survivors with
 //                 ballot/popc into a warp queue and runs the base-2 strong
 //                 PRP test 32 candidates at a time, one atomic per warp for the
 //                 output slots.
 //   k_wieferich / k_wallsunsun   the two reference test kernels.
-//   k_test_prps   both tests in one pass over the PRP list.
+//   k_test_prps   both tests in one pass over the PRP list (warps pull work
+//                 from a cursor, or stride).
 //   k_digits      per-prime canonical digits (verification only).
 #pragma once
 
