@@ -179,6 +179,7 @@ BatchArgs make_args(BatchState &b, u32 n, u64 n_tiles) {
     a.hit_count = b.d_hit_count;
     a.hit_capacity = b.hit_cap;
     a.overflow = b.d_overflow;
+    a.deep = deep_rows_device();  // callers check it before launching
     return a;
 }
 
@@ -228,6 +229,7 @@ int run_batch(ww_ctx *ctx, BatchState &b, const ww_unit *units, uint32_t n, cons
     rc = launch_grid(e, dev, &grid);
     if (rc) return rc;
     const BatchArgs a = make_args(b, n, acc);
+    if (!a.deep) return WW_ERR_CUDA;
 
     cudaGraph_t g = nullptr;
     WW_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -682,6 +684,8 @@ int ww_server_step(ww_ctx *ctx, ww_request_result *done, uint32_t cap, uint32_t 
     a.hit_count = s.d_hit_count;
     a.hit_capacity = s.cfg.max_hits;
     a.overflow = s.d_overflow;
+    a.deep = deep_rows_device();
+    if (!a.deep) return WW_ERR_CUDA;
     const int grid = std::min<int>(s.grid, (int)a.budget);
     s.e->serve_kernel<<<grid, s.e->threads, s.e->smem, st>>>(a);
     WW_CU(cudaGetLastError());

@@ -50,6 +50,7 @@ struct BatchArgs {
     u32 *hit_count;
     u32 hit_capacity;
     u32 *overflow;           // bit 1: hit list overflow, bit 0: a PRP buffer overflowed
+    const DeepRow *deep;     // the deep-sieve table (deep_rows_device())
 };
 
 template <int SEG_WORDS, int THREADS, int PPT>
@@ -224,7 +225,7 @@ __global__ void __launch_bounds__(Cfg::kThreads) k_tiles(BatchArgs a) {
 
         // ---- deep sieve 113 < r < 2^WW_DEEP_BITS, sparing possible pseudoprimes
         const u64 nbase = b0 + 1;
-        deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, Cfg::kThreads);
+        deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, Cfg::kThreads, a.deep);
         __syncthreads();
 
         // ---- chunks of 32 words, taken dynamically by the warps

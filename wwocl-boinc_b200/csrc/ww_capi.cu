@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <thread>
 
@@ -93,6 +94,38 @@ int wallsunsun_grid() {
 
 }  // namespace
 
+// The deep-sieve table: the one device copy in the library (every kernel
+// that sieves gets its address).
+#define WW_DEEP_ROWD(r, o, rinv, mr, mo) {r, o, rinv, mr, mo},
+__device__ const DeepRow g_deep_rows[kDeepUse] = {WW_DEEP_ROWS(WW_DEEP_ROWD)};
+#undef WW_DEEP_ROWD
+
+namespace ww {
+// Device address of g_deep_rows on the current device (looked up once per
+// device), or nullptr with the error set.
+const DeepRow *deep_rows_device() {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mutex;
+    static const DeepRow *addr[kMaxDevices] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        set_err("no usable current device");
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mutex);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_deep_rows);
+        if (e != cudaSuccess) {
+            set_err("deep-sieve table: %s", cudaGetErrorString(e));
+            return nullptr;
+        }
+        addr[dev] = static_cast<const DeepRow *>(p);
+    }
+    return addr[dev];
+}
+}  // namespace ww
+
 int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime, uint64_t *g_invert,
                  uint32_t *primecount, uint64_t capacity, uint32_t *overflow, void *stream, u64 *cursor);
 
@@ -171,8 +204,10 @@ int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prim
     const uint64_t slots = (uint64_t)sm_count() * (uint64_t)per_sm;
     const uint64_t grid = nseg < slots ? nseg : slots;
     PrpOut out{(u64 *)g_prime, (u64 *)g_invert, primecount, capacity, overflow};
+    const DeepRow *deep = deep_rows_device();
+    if (!deep) return WW_ERR_CUDA;
     if (cursor) WW_CU(cudaMemsetAsync(cursor, 0, sizeof(u64), as_stream(stream)));
-    k_sieve_prp<<<(unsigned)grid, kSieveThreads, 0, as_stream(stream)>>>(low, high, nseg, out, cursor);
+    k_sieve_prp<<<(unsigned)grid, kSieveThreads, 0, as_stream(stream)>>>(low, high, nseg, out, cursor, deep);
     WW_CHECK_LAUNCH();
     return WW_OK;
 }

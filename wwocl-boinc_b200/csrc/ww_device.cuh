@@ -92,9 +92,9 @@ __device__ __forceinline__ void step_hit(u32 &j0) {
 // ------------------------------------------------------------- deep sieve
 // (the scheme is described in ww_deep.cuh)
 
-#define WW_DEEP_ROWD(r, o, rinv, mr, mo) {r, o, rinv, mr, mo},
-static __device__ const DeepRow kDeepDev[WW_DEEP_COUNT] = {WW_DEEP_ROWS(WW_DEEP_ROWD)};
-#undef WW_DEEP_ROWD
+// The deep-sieve table lives once in device memory (ww_capi.cu); kernels
+// get its address as an argument.  Host code asks for it per device.
+const DeepRow *deep_rows_device();
 
 // Mark the odd multiples n = r*k of the deep primes in the segment, except
 // those with k = 1 (mod ord_r(2)) (ww_deep.cuh says why).  The smallest
@@ -104,10 +104,11 @@ static __device__ const DeepRow kDeepDev[WW_DEEP_COUNT] = {WW_DEEP_ROWS(WW_DEEP_
 // holds the others at the next barrier.
 constexpr int kDeepWarpPrimes = 512;
 
-__device__ __forceinline__ void deep_mark(u64 first, u32 nvalid, u32 *bitmap, int tid, int nthreads) {
+__device__ __forceinline__ void deep_mark(u64 first, u32 nvalid, u32 *bitmap, int tid, int nthreads,
+                                          const DeepRow *__restrict__ deep) {
     const int lane = tid & 31, warp = tid >> 5, nwarps = nthreads >> 5;
     for (int i = warp; i < kDeepWarpPrimes && i < kDeepUse; i += nwarps) {
-        const DeepRow e = kDeepDev[i];
+        const DeepRow e = deep[i];
         u32 j0, km0;
         deep_start(first, e, j0, km0);
         u32 km = (km0 + 2u * (u32)lane) % e.o;
@@ -119,7 +120,7 @@ __device__ __forceinline__ void deep_mark(u64 first, u32 nvalid, u32 *bitmap, in
         }
     }
     for (int i = kDeepWarpPrimes + tid; i < kDeepUse; i += nthreads) {
-        const DeepRow e = kDeepDev[i];
+        const DeepRow e = deep[i];
         u32 j, km;
         deep_start(first, e, j, km);
         for (; j < nvalid; j += e.r) {

@@ -27,7 +27,8 @@ namespace ww {
 // With a segment cursor (zeroed before the launch) the CTAs take segments
 // one at a time from it; without one (the kernel-shaped entry point) they
 // stride over the segments.
-__global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out, u64 *cursor) {
+__global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out, u64 *cursor,
+                                                             const DeepRow *deep) {
     __shared__ u32 bitmap[kSegWords];
     __shared__ u32 queue[kSieveWarps][kQueueCap];
     __shared__ u32 s_chunk;
@@ -75,7 +76,7 @@ __global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64
 
         // ---- deep sieve 113 < r < 2^WW_DEEP_BITS, sparing possible pseudoprimes
         const u64 nbase = b0 + seg_off + 1;
-        deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, kSieveThreads);
+        deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, kSieveThreads, deep);
         __syncthreads();
 
         // ---- warps take 32-word chunks dynamically (so they reach the next

@@ -188,6 +188,8 @@ extern "C" int ww_batch_run_noalloc(const ww_unit *units, uint32_t n, ww_unit_re
     a.hit_count = &s->hit_count;
     a.hit_capacity = kNoAllocMaxHits;
     a.overflow = &s->overflow;
+    a.deep = deep_rows_device();  // the library's constant table, no allocation
+    if (!a.deep) return WW_ERR_CUDA;
     if (acc)
         k_tiles<NoAllocCfg, false><<<d.grid, NoAllocCfg::kThreads, batch_smem_bytes<NoAllocCfg>(), st>>>(a);
     k_noalloc_finish<<<32, 256, 0, st>>>(s, n, out, hits, hit_unit, hit_cap, hit_count);
