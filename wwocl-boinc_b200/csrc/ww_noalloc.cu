@@ -17,9 +17,9 @@
 // keeps the previous call's contents, so each call clears what must start
 // at zero, and calls whose GPU work overlaps (on different streams, or from
 // different host threads) race on it -- order them on one stream.  The
-// first call on each device does a one-time set-up (the array's device
-// address and the kernel's shared-memory attribute), which should come
-// before any stream capture.
+// first call on each device does a one-time set-up (the device addresses of
+// the array and of the library's deep-sieve table, and the kernel's
+// shared-memory attribute), which should come before any stream capture.
 #include <cuda_runtime.h>
 
 #include <cstring>
