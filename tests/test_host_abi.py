@@ -190,3 +190,41 @@ def test_deep_sieve_spares_pseudoprimes_with_deep_factors(ww, oracle):
     # 49141 is spared by both of its factors; it must reach the PRP test once
     cand, spared = ww.selftest_candidates(49141 - 10, 49141 + 10)
     assert spared >= 2 and cand.tolist().count(49141) == 1
+
+
+def test_deep_table_rows_are_exact():
+    """Every row of the generated deep-sieve table: r prime (113 < r), o the
+    exact multiplicative order of 2 mod r, r^-1 mod 2^64, floor(2^64 / r),
+    floor(2^64 / o); rows ascending; the band counts add up."""
+    import re
+
+    from conftest import PKG
+
+    text = (PKG / "csrc" / "ww_deep_table.h").read_text()
+    counts = {int(b): int(n) for b, n in re.findall(r"#define WW_DEEP_COUNT_(\d+) (\d+)", text)}
+    rows = [tuple(int(v, 0) for v in m) for m in
+            re.findall(r"X\((\d+)u, (\d+)u, (0x[0-9a-f]+)ull, (0x[0-9a-f]+)ull, (0x[0-9a-f]+)ull\)", text)]
+    assert len(rows) == max(counts.values())
+    for b, n in counts.items():
+        assert sum(1 for r in rows if r[0] < (1 << b)) == n, b
+    limit = 1 << max(counts)
+    sieve = bytearray([1]) * limit
+    sieve[0:2] = b"\0\0"
+    for i in range(2, int(limit ** 0.5) + 1):
+        if sieve[i]:
+            sieve[i * i::i] = bytearray(len(range(i * i, limit, i)))
+    assert [r[0] for r in rows] == [p for p in range(114, limit) if sieve[p]]
+    M = 1 << 64
+    for r, o, rinv, mr, mo in rows:
+        assert (r * rinv) % M == 1 and mr == M // r and mo == M // o, r
+        assert (r - 1) % o == 0 and pow(2, o, r) == 1, r
+        # o is the order: no proper divisor o/q with q prime works
+        x, q = o, 2
+        while q * q <= x:
+            if x % q == 0:
+                assert pow(2, o // q, r) != 1, r
+                while x % q == 0:
+                    x //= q
+            q += 1
+        if x > 1:
+            assert pow(2, o // x, r) != 1, r
