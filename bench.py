@@ -9,7 +9,13 @@ One step = one fused Wieferich + Wall-Sun-Sun launch over the whole list
 (`value`: list resident in HBM; `e2e`: the same step through the C ABI with
 the list copied from pinned host memory and the counters read back, every
 step).  Under torchrun each rank tests its own list (seed 7 + rank): weak
-scaling, no data-path collective.  Rank 0 prints one JSON line.
+scaling, no data-path collective.  Rank 0 prints one JSON line, which at
+N = 1 also carries: `roofline` (the test kernel against the measured
+integer-multiply chain peak), `cpu_baseline` (the reference's own CPU code on
+the host cores), `range_pipeline` (the plain path over the 2^34-wide range
+below 2^64, checksum against the reference), `batched_vs_plain` (the uneven
+mix: batched engine vs one launch sequence per range, vs one program run per
+range) and `serving` (Poisson request stream, p50/p99 latency).
 """
 from __future__ import annotations
 
