@@ -39,6 +39,8 @@ RANGES = [
     ("wieferich_special_window", 2276306935816523 - 1_000_000, 2276306935816523 + 1_000_000),
     ("wss_special_window", 338772621946054253, 338772621946054253 + 2_000_000),
     ("mid_2p48", 2**48, 2**48 + 3_000_000),
+    ("cross_2p62", 2**62 - 1_000_000, 2**62 + 1_000_000),
+    ("cross_2p63", 2**63 - 1_000_000, 2**63 + 1_000_000),
 ]
 
 PRP_RANGES = [
@@ -84,6 +86,19 @@ def prime_samples(o: Oracle) -> dict[str, np.ndarray]:
             top.append(n)
         n -= 2
     out["near_2p64"] = np.array(top, dtype=np.uint64)
+    for name, centre in (("near_2p63", 2**63), ("near_2p62", 2**62)):
+        side = []
+        n = centre - 1
+        while len(side) < 800:
+            if o.is_prp(n):
+                side.append(n)
+            n -= 2
+        n = centre + 1
+        while len(side) < 1600:
+            if o.is_prp(n):
+                side.append(n)
+            n += 2
+        out[name] = np.array(side, dtype=np.uint64)
     rnd = []
     while len(rnd) < 4000:
         c = int(rng.integers(0, 2**63, dtype=np.uint64)) * 2 + 1

@@ -88,7 +88,8 @@ def test_sieve_prp_list_inverse(ww):
 
 @pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("name", ["small_3e6", "cross_2p32", "near_top_2e6", "wieferich_special_window",
-                                  "wss_special_window", "mid_2p48", "config1_5e7", "top_1e8"])
+                                  "wss_special_window", "mid_2p48", "config1_5e7", "top_1e8", "cross_2p62",
+                                  "cross_2p63"])
 def test_pipeline_matches_reference(ctx, ref_ranges, name, fused):
     r = ref_ranges[name]
     got = ctx.run_range(r["lo"], r["hi"], fused=fused)

@@ -41,7 +41,8 @@ def test_tests_txt_hits_in_windows(oracle, tests_txt):
 
 
 @pytest.mark.parametrize("name", ["small_3e6", "cross_2p32", "near_top_2e6", "wieferich_special_window",
-                                  "wss_special_window", "mid_2p48", "config1_5e7", "top_1e8"])
+                                  "wss_special_window", "mid_2p48", "config1_5e7", "top_1e8", "cross_2p62",
+                                  "cross_2p63"])
 def test_oracle_ranges_match_reference(oracle, ref_ranges, name):
     r = ref_ranges[name]
     summ, _, _ = oracle.scan_range(r["lo"], r["hi"])
