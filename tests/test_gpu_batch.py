@@ -22,7 +22,8 @@ def _alone(ctx, lo, hi):
 
 def test_small_units_match_oracle(ww, ctx, oracle):
     units = [(127, 1_000_000), (4_294_000_000, 4_295_500_000), (2**64 - 2**35, 2**64 - 2**35 + 700_001),
-             (2276306935816523 - 5000, 2276306935816523 + 5000), (1000, 1000), (2**64 - 1_000_001, 2**64 - 1)]
+             (2276306935816523 - 5000, 2276306935816523 + 5000), (1000, 1000), (2**64 - 1_000_001, 2**64 - 1),
+             (2**63 - 500_001, 2**63 + 499_999), (2**62 - 300_000, 2**62 + 300_000)]
     b = ww.Batch(ctx)
     got = b.run(units)
     hits = b.hits()

@@ -121,7 +121,7 @@ def test_count_prps_matches_reference(ctx, ref_ranges):
     import json
     from pathlib import Path
 
-    for name in ("small_3e6", "config1_5e7", "cross_2p32", "near_top_2e6", "top_1e8"):
+    for name in ("small_3e6", "config1_5e7", "cross_2p32", "cross_2p63", "near_top_2e6", "top_1e8"):
         r = ref_ranges[name]
         assert ctx.count_prps(r["lo"], r["hi"]) == r["prp_count"], name
     long = json.loads((Path(__file__).resolve().parent / "golden" / "ref_long.json").read_text())["config3"]
