@@ -71,3 +71,26 @@ def test_bad_unit_is_rejected(ww, ctx):
     b = ww.Batch(ctx)
     with pytest.raises(ww.WWError):
         b.run([(100, 1000)])
+
+
+def test_one_and_two_number_ranges(ww, ctx, oracle):
+    """Ranges one or two numbers wide on a Wieferich special instance, a WSS
+    special instance, a base-2 strong pseudoprime (49141), the first allowed
+    start, the largest 64-bit prime and the last numbers below 2^64: the
+    batched engine, the plain path and the GPU count agree with the oracle,
+    hits included."""
+    units = [(2276306935816523, 2276306935816524), (338772621946054253, 338772621946054255),
+             (49141, 49142), (127, 128), (127, 129), (2**64 - 59, 2**64 - 58), (2**64 - 3, 2**64 - 1),
+             (2**64 - 2, 2**64 - 1), (1_000_003, 1_000_004), (1_000_004, 1_000_005)]
+    b = ww.Batch(ctx)
+    got = b.run(units)
+    hits = b.hits()
+    for i, (lo, hi) in enumerate(units):
+        want, _, whits = oracle.scan_range(lo, hi, hit_cap=1000)
+        assert got[i]["checksum"] == want["checksum"] and got[i]["prp_count"] == want["prp_count"], (lo, hi)
+        assert sorted(h[1:] for h in hits if h[0] == i) == sorted(whits), (lo, hi)
+        alone = ctx.run_range(lo, hi)
+        assert alone["checksum"] == want["checksum"] and alone["total_prp_count"] == want["prp_count"], (lo, hi)
+        assert sorted(alone["hits"]) == sorted(whits), (lo, hi)
+        assert ctx.count_prps(lo, hi) == want["prp_count"], (lo, hi)
+    assert got[0]["hits"] == 1 and got[1]["hits"] == 1 and got[2]["prp_count"] == 1 and got[5]["prp_count"] == 1

@@ -317,8 +317,13 @@ class Context:
         check(_L.ww_clear_segment(self.h), "ww_clear_segment")
 
     def sieve_prp(self, start: int, stop: int) -> None:
-        """getsegprimes over [start, stop) after the wheel alignment of start."""
-        ks, idx = find_wheel_offset(start)
+        """getsegprimes over [start, stop) after the wheel alignment of start
+        (nothing to do when no number from start on is prime to 30, which
+        happens only in the last few numbers below 2^64)."""
+        s, i = C.c_uint64(start), C.c_int32(0)
+        if _L.ww_find_wheel_offset(C.byref(s), C.byref(i)) != 0:
+            return
+        ks, idx = int(s.value), int(i.value)
         if ks >= stop:
             return
         check(_L.ww_sieve_prp(self.h, ks, stop, idx), "ww_sieve_prp")
