@@ -94,3 +94,25 @@ def test_one_and_two_number_ranges(ww, ctx, oracle):
         assert sorted(alone["hits"]) == sorted(whits), (lo, hi)
         assert ctx.count_prps(lo, hi) == want["prp_count"], (lo, hi)
     assert got[0]["hits"] == 1 and got[1]["hits"] == 1 and got[2]["prp_count"] == 1 and got[5]["prp_count"] == 1
+
+
+def test_hit_overflow_keeps_results(ww, ctx, oracle):
+    """More hits than the batch's hit buffer holds ([127, 2e6) has thousands
+    of special instances): the overflow is reported, every range's checksum
+    and PRP count is still right, and the records that fit are real hits."""
+    units = [(127, 1_000_000), (1_000_000, 2_000_000)]
+    with ww.Context(0, max_prps=1 << 20, max_hits=15000) as small:  # a fresh batch: its hit buffer only grows
+        b = ww.Batch(small, max_hits=64)
+        got = b.run(units)
+        assert b.hit_overflow and b.hit_count > 64
+        allhits = set()
+        for i, (lo, hi) in enumerate(units):
+            want, _, whits = oracle.scan_range(lo, hi, hit_cap=100000)
+            assert got[i]["checksum"] == want["checksum"] and got[i]["prp_count"] == want["prp_count"]
+            assert got[i]["hits"] == want["gpu_results"]
+            allhits |= {(i, *h) for h in whits}
+        kept = b.hits()
+        assert len(kept) == 64 and all(h in allhits for h in kept)
+        # a batch whose hits fit clears the flag
+        b.run([(10**15, 10**15 + 10**6)])
+        assert not b.hit_overflow

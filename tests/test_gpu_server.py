@@ -84,3 +84,20 @@ def test_admission_waits_for_memory(ww, ctx):
             break
     assert len(done) == len(reqs) and seen_active <= 2
     srv.close()
+
+
+def test_hit_overflow_is_reported_per_request(ww, ctx):
+    """A step whose hit records overflow loses records of the requests active
+    in it: each such request reports WW_ERR_HIT_OVERFLOW when it finishes, in
+    whatever later step that is, with its checksum and PRP count still right;
+    a request whose hits all fit reports OK."""
+    reqs = [(1, 127, 2_000_000), (2, 10**15, 10**15 + 10**6)]
+    srv = ww.Server(ctx, prp_pool_bytes=1 << 28, max_active=4, epoch_tiles=2, max_hits=16)
+    srv.submit(reqs)
+    done = {r["id"]: r for r in srv.drain()}
+    srv.close()
+    assert done[1]["status"] == -4 and done[1]["hits"] > 16
+    assert done[2]["status"] == 0
+    for rid, a, b in reqs:
+        ref = ctx.run_range(a, b)
+        assert (done[rid]["checksum"], done[rid]["prp_count"]) == (ref["checksum"], ref["total_prp_count"])

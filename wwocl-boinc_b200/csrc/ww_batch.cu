@@ -707,7 +707,6 @@ int ww_server_step(ww_ctx *ctx, ww_request_result *done, uint32_t cap, uint32_t 
                     ww_hit{s.h_hit_p[i], s.h_hit_res[i], s.h_hit_rem[i], s.h_hit_quot[i], 0});
         }
     }
-    const bool hit_overflow = (s.h_counts[1] & 2) != 0;
 
     // ---- finished requests
     const double t = mono_s();
@@ -723,7 +722,13 @@ int ww_server_step(ww_ctx *ctx, ww_request_result *done, uint32_t cap, uint32_t 
             r.prp_count = u.prp_count;
             r.prps_stored = u.prp_out ? std::min(u.prp_written, u.prp_cap) : 0;
             r.hits = u.hits;
-            r.status = hit_overflow ? WW_ERR_HIT_OVERFLOW : (u.prp_written > u.prp_cap && u.prp_out ? WW_ERR_PRP_OVERFLOW : WW_OK);
+            // a step whose hit records overflowed loses records of every
+            // request active in it: compare the request's own count of hits
+            // with the records it got, over all of its steps
+            const auto it = s.hits.find(sl.r.id);
+            const size_t kept = it == s.hits.end() ? 0 : it->second.size();
+            r.status = kept < u.hits ? WW_ERR_HIT_OVERFLOW
+                                     : (u.prp_written > u.prp_cap && u.prp_out ? WW_ERR_PRP_OVERFLOW : WW_OK);
             r.t_submit = sl.t_submit;
             r.t_admit = sl.t_admit;
             r.t_done = t;

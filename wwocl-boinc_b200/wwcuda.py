@@ -468,9 +468,15 @@ class Batch:
         check(_L.ww_batch_submit(self.ctx.h, self._u, self._n), "ww_batch_submit")
 
     def collect(self) -> list[dict]:
+        """Per-range results.  When the hit records overflowed their buffer
+        the results are still complete; hit_overflow is then True and
+        hits() returns the records that fit."""
         out = (UnitResult * max(self._n, 1))()
         hc = C.c_uint32(0)
-        check(_L.ww_batch_collect(self.ctx.h, out, self._n, C.byref(hc)), "ww_batch_collect")
+        rc = _L.ww_batch_collect(self.ctx.h, out, self._n, C.byref(hc))
+        self.hit_overflow = rc == -4
+        if rc != WW_OK and not self.hit_overflow:
+            raise WWError(rc, "ww_batch_collect")
         self.hit_count = hc.value
         return [dict(checksum=r.checksum, prp_count=r.prp_count, hits=r.hits, tiles_done=r.tiles_done)
                 for r in out[: self._n]]
@@ -484,7 +490,9 @@ class Batch:
         arr = (Hit * cap)()
         units = (C.c_uint32 * cap)()
         n = C.c_uint32(0)
-        check(_L.ww_batch_hits(self.ctx.h, arr, units, cap, C.byref(n)), "ww_batch_hits")
+        rc = _L.ww_batch_hits(self.ctx.h, arr, units, cap, C.byref(n))
+        if rc != WW_OK and rc != -4:  # -4: more hits than the buffer held; return those that fit
+            raise WWError(rc, "ww_batch_hits")
         return [(units[i], arr[i].p, arr[i].result, arr[i].rem, arr[i].quot) for i in range(min(n.value, cap))]
 
 
