@@ -94,6 +94,9 @@ def test_one_and_two_number_ranges(ww, ctx, oracle):
         assert sorted(alone["hits"]) == sorted(whits), (lo, hi)
         assert ctx.count_prps(lo, hi) == want["prp_count"], (lo, hi)
     assert got[0]["hits"] == 1 and got[1]["hits"] == 1 and got[2]["prp_count"] == 1 and got[5]["prp_count"] == 1
+    # an empty batch, then a batch again
+    assert b.run([]) == []
+    assert b.run(units[:1])[0]["checksum"] == got[0]["checksum"]
 
 
 def test_hit_overflow_keeps_results(ww, ctx, oracle):

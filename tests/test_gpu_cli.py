@@ -91,3 +91,16 @@ def test_debug_prints_kernel_profile_and_counters(tests_txt, tmp_path):
     assert "PRPs tested since last checkpoint:" in out
     lines = (tmp_path / "results-WW.txt").read_text().splitlines()
     assert lines == c["hits"] + [c["checksum"]]
+
+
+def test_testprimes_checks_every_segment(ref_ranges, tmp_path):
+    """-testprimes (main.cpp:1177-1183,1732-1735): every segment's GPU PRP
+    list, pseudoprimes set aside, equals the CPU prime list; the range
+    [127, 3e6) holds base-2 strong pseudoprimes (1373653 = 829 * 1657 among
+    them), and the run still ends with the reference checksum."""
+    r = ref_ranges["small_3e6"]
+    out = run([str(r["lo"]), str(r["hi"]), "-testprimes", "-ckpt", "1e6"], tmp_path)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.count("GPU primes match CPU") >= 3
+    lines = (tmp_path / "results-WW.txt").read_text().splitlines()
+    assert lines[-1] == r["checksum"]
