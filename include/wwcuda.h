@@ -288,6 +288,9 @@ typedef struct {
 
 int ww_server_open(ww_ctx *ctx, const ww_server_cfg *cfg);
 int ww_server_close(ww_ctx *ctx);
+/* Queue requests (host side, any time).  All or none: WW_ERR_ARG for a bad
+ * range, WW_ERR_NOMEM for a request whose PRP list could never fit the pool
+ * (store_prps), and then no request of the call is queued. */
 int ww_server_submit(ww_ctx *ctx, const ww_request *reqs, uint32_t n);
 /* Admit, run one epoch, collect finished requests into done[0..*ndone). */
 int ww_server_step(ww_ctx *ctx, ww_request_result *done, uint32_t cap, uint32_t *ndone);

@@ -83,6 +83,16 @@ def test_admission_waits_for_memory(ww, ctx):
         if q == 0 and a == 0:
             break
     assert len(done) == len(reqs) and seen_active <= 2
+    # a request that could never fit the pool is refused at submission, with
+    # the rest of its call, and the server goes on serving
+    big = (99, 10**15, 10**15 + 10**9)
+    with pytest.raises(ww.WWError) as err:
+        srv.submit([reqs[0], big])
+    assert err.value.status == -6
+    assert srv.status()[0] == 0
+    srv.submit([(100, reqs[0][1], reqs[0][2])])
+    again = srv.drain()
+    assert len(again) == 1 and again[0]["status"] == 0
     srv.close()
 
 

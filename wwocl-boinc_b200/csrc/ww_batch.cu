@@ -590,12 +590,20 @@ int ww_server_submit(ww_ctx *ctx, const ww_request *reqs, uint32_t n) {
     ServerState *sv = ctx ? ctx_server(ctx) : nullptr;
     if (!sv) return set_err("server not open"), WW_ERR_STATE;
     if (!reqs && n) return set_err("null requests"), WW_ERR_ARG;
-    const double t = mono_s();
+    // check every request first, so a refused call queues none of them
     for (uint32_t i = 0; i < n; ++i) {
         if (reqs[i].end <= reqs[i].start || reqs[i].start < 127)
             return set_err("request %llu: bad range", (unsigned long long)reqs[i].id), WW_ERR_ARG;
-        sv->queue.push_back(ServerReq{reqs[i], t});
+        // a PRP list that could never fit the pool would wait at the head of
+        // the queue for ever
+        if (sv->cfg.store_prps && ww_prp_count_bound(reqs[i].start, reqs[i].end) * 8 > sv->cfg.prp_pool_bytes)
+            return set_err("request %llu needs %llu bytes of PRP pool, the pool has %llu",
+                           (unsigned long long)reqs[i].id,
+                           (unsigned long long)(ww_prp_count_bound(reqs[i].start, reqs[i].end) * 8),
+                           (unsigned long long)sv->cfg.prp_pool_bytes), WW_ERR_NOMEM;
     }
+    const double t = mono_s();
+    for (uint32_t i = 0; i < n; ++i) sv->queue.push_back(ServerReq{reqs[i], t});
     return WW_OK;
 }
 
