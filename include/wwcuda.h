@@ -85,6 +85,11 @@ int ww_launch_clearn(uint32_t *primecount, void *stream);
 int ww_launch_clearresult(uint64_t *checksum, uint32_t *resultcount, uint64_t *totalprimecount,
                           uint32_t *primecount, void *stream);
 
+/* The four launchers below take work from a cursor that the library lends
+ * to the calling stream (a pool of 64 per device). A stream being captured
+ * into a CUDA graph, or a launch that finds every cursor busy, splits the
+ * work statically instead, with the same results. */
+
 /* getsegprimes (getsegprimes.cl:228-301): every base-2 strong probable prime
  * in [low, high) with no prime factor <= 113 is appended to g_prime, with
  * q = p^-1 mod 2^64 in g_invert, counted in primecount[0].  low must be the

@@ -180,43 +180,107 @@ def test_hit_overflow_is_reported(ww):
         assert e.value.status == -4
 
 
-def test_kernel_shaped_launchers_on_torch_memory(ww, ref_ranges):
+class _KernelSequence:
     """The reference kernel sequence clearresult, clearn, getsegprimes,
-    wieferich, wallsunsun on caller-owned device memory and stream."""
+    wieferich, wallsunsun over one range, on caller-owned device memory."""
+
+    def __init__(self, ww, r, cap=1 << 18, nres=15000):
+        import torch
+
+        dev = torch.device("cuda", 0)
+        self.ww, self.L, self.r, self.cap, self.nres = ww, ww.lib(), r, cap, nres
+        e = lambda n, dt: torch.empty(n, dtype=dt, device=dev)  # noqa: E731
+        self.prime, self.inv, self.one = e(cap, torch.int64), e(cap, torch.int64), e(2 * cap, torch.int64)
+        self.sp, self.rem, self.quot, self.res = (e(nres, torch.int64), e(nres, torch.int32), e(nres, torch.int32),
+                                                  e(nres, torch.int32))
+        self.cks, self.total = e(1, torch.int64), e(1, torch.int64)
+        self.rc, self.pc, self.ovf = e(1, torch.int32), e(2, torch.int32), torch.zeros(1, dtype=torch.int32,
+                                                                                         device=dev)
+
+    def launch(self, st):
+        ww, L, r, cap, nres = self.ww, self.L, self.r, self.cap, self.nres
+        P = lambda t: t.data_ptr()  # noqa: E731
+        start, idx = ww.find_wheel_offset(r["lo"])
+        ww.check(L.ww_launch_clearresult(P(self.cks), P(self.rc), P(self.total), P(self.pc), st), "clearresult")
+        ww.check(L.ww_launch_clearn(P(self.pc), st), "clearn")
+        ww.check(L.ww_launch_getsegprimes(start, r["hi"], idx, P(self.prime), P(self.inv), P(self.pc), cap,
+                                          P(self.ovf), st), "gsp")
+        ww.check(L.ww_launch_wieferich(P(self.pc), P(self.prime), P(self.inv), P(self.one), P(self.sp), P(self.rem),
+                                       P(self.quot), P(self.res), P(self.cks), P(self.rc), P(self.total), cap, nres,
+                                       P(self.ovf), st), "wieferich")
+        ww.check(L.ww_launch_wallsunsun(P(self.pc), P(self.prime), P(self.inv), P(self.one), P(self.sp),
+                                        P(self.rem), P(self.quot), P(self.res), P(self.cks), P(self.rc), cap, nres,
+                                        P(self.ovf), st), "wallsunsun")
+
+    def check(self, label=""):
+        r = self.r
+        assert int(self.ovf.item()) == 0, label
+        assert int(self.total.item()) == r["prp_count"], label
+        assert "%016X" % (int(self.cks.item()) % 2**64) == r["checksum"], label
+        assert int(self.rc.item()) == r["cpu_results"], label
+
+
+def test_kernel_shaped_launchers_on_torch_memory(ww, ref_ranges):
+    """The reference kernel sequence on caller-owned device memory and stream."""
     import torch
 
-    L = ww.lib()
-    r = ref_ranges["cross_2p32"]
-    dev = torch.device("cuda", 0)
-    cap, nres = 1 << 18, 15000
-    prime = torch.empty(cap, dtype=torch.int64, device=dev)
-    inv = torch.empty(cap, dtype=torch.int64, device=dev)
-    one = torch.empty(2 * cap, dtype=torch.int64, device=dev)
-    sp = torch.empty(nres, dtype=torch.int64, device=dev)
-    rem = torch.empty(nres, dtype=torch.int32, device=dev)
-    quot = torch.empty(nres, dtype=torch.int32, device=dev)
-    res = torch.empty(nres, dtype=torch.int32, device=dev)
-    cks = torch.zeros(1, dtype=torch.int64, device=dev)
-    total = torch.zeros(1, dtype=torch.int64, device=dev)
-    rc = torch.zeros(1, dtype=torch.int32, device=dev)
-    pc = torch.zeros(2, dtype=torch.int32, device=dev)
-    ovf = torch.zeros(1, dtype=torch.int32, device=dev)
-    s = torch.cuda.Stream(dev)
-    st = s.cuda_stream
-    P = lambda t: t.data_ptr()  # noqa: E731
-    start, idx = ww.find_wheel_offset(r["lo"])
-    ww.check(L.ww_launch_clearresult(P(cks), P(rc), P(total), P(pc), st), "clearresult")
-    ww.check(L.ww_launch_clearn(P(pc), st), "clearn")
-    ww.check(L.ww_launch_getsegprimes(start, r["hi"], idx, P(prime), P(inv), P(pc), cap, P(ovf), st), "gsp")
-    ww.check(L.ww_launch_wieferich(P(pc), P(prime), P(inv), P(one), P(sp), P(rem), P(quot), P(res), P(cks),
-                                   P(rc), P(total), cap, nres, P(ovf), st), "wieferich")
-    ww.check(L.ww_launch_wallsunsun(P(pc), P(prime), P(inv), P(one), P(sp), P(rem), P(quot), P(res), P(cks),
-                                    P(rc), cap, nres, P(ovf), st), "wallsunsun")
+    seq = _KernelSequence(ww, ref_ranges["cross_2p32"])
+    s = torch.cuda.Stream(torch.device("cuda", 0))
+    seq.launch(s.cuda_stream)
     s.synchronize()
-    assert int(ovf.item()) == 0
-    assert int(total.item()) == r["prp_count"]
-    assert "%016X" % (int(cks.item()) % 2**64) == r["checksum"]
-    assert int(rc.item()) == r["cpu_results"]
+    seq.check()
+
+
+def test_kernel_shaped_launchers_on_many_streams(ww, ref_ranges):
+    """The kernel-shaped launchers lend each stream a work cursor from a
+    fixed pool of 64 per device.  96 distinct streams, all queued before any
+    finishes: streams that find no free slot take the static split, the
+    second round reuses slots whose work has completed, and every stream's
+    results equal the reference's.  The default stream runs one too."""
+    import torch
+
+    cudart = pytest.importorskip("cuda.bindings.runtime")
+    dev = torch.device("cuda", 0)
+    names = ["cross_2p32", "wieferich_special_window", "near_top_2e6", "cross_2p63", "wss_special_window"]
+    handles = []
+    try:
+        for _ in range(96):
+            err, h = cudart.cudaStreamCreateWithFlags(cudart.cudaStreamNonBlocking)
+            assert err == cudart.cudaError_t.cudaSuccess
+            handles.append(h)
+        seqs = [_KernelSequence(ww, ref_ranges[names[i % len(names)]], cap=1 << 17, nres=64)
+                for i in range(len(handles))]
+        default = _KernelSequence(ww, ref_ranges["mid_2p48"], cap=1 << 17, nres=64)
+        torch.cuda.synchronize(dev)
+        for rnd in range(2):
+            for h, q in zip(handles, seqs):
+                q.launch(int(h))
+            default.launch(0)
+            torch.cuda.synchronize(dev)
+            for i, q in enumerate(seqs):
+                q.check("round %d stream %d" % (rnd, i))
+            default.check("default stream")
+    finally:
+        torch.cuda.synchronize(dev)
+        for h in handles:
+            cudart.cudaStreamDestroy(h)
+
+
+def test_kernel_shaped_launchers_under_graph_capture(ww, ref_ranges):
+    """Launches captured into a CUDA graph (no cursor there) replay to the
+    reference's results, twice."""
+    import torch
+
+    seq = _KernelSequence(ww, ref_ranges["wieferich_special_window"], cap=1 << 17, nres=64)
+    s = torch.cuda.Stream(torch.device("cuda", 0))
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s, capture_error_mode="relaxed"):
+        seq.launch(s.cuda_stream)
+    for _ in range(2):
+        seq.ovf.zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        seq.check()
 
 
 def test_bad_arguments_are_rejected(ww):

@@ -66,9 +66,9 @@ int wheel_index_of(uint64_t n) {
     }
 }
 
-// One full wave of resident CTAs: the test kernels split the list evenly
-// over the grid (grid-stride loop), so a grid above the resident count would
-// leave its last CTAs running as a thinly occupied second wave.
+// One full wave of resident CTAs: the test kernels take work from a cursor
+// (or, without one, split the list evenly over the grid), so a grid above
+// the resident count would only add CTAs that wait for a free slot.
 template <class Kernel>
 int resident_grid(Kernel k, int threads) {
     int per_sm = 0;
@@ -126,6 +126,87 @@ const DeepRow *deep_rows_device() {
 }
 }  // namespace ww
 
+// Work cursors for the kernel-shaped launchers, whose callers pass no scratch:
+// a pool per device, each slot (one 128-byte line, so the slots' atomics do
+// not share a line) lent to one stream at a time.
+constexpr int kLaunchCursorSlots = 64;
+constexpr int kLaunchCursorStride = 16;
+__device__ u64 g_launch_cursors[kLaunchCursorSlots * kLaunchCursorStride];
+
+namespace {
+
+// The host side of g_launch_cursors, one per device, shared by every
+// launcher (one lock, one owner table).
+struct CursorPool {
+    enum State : unsigned char { kFree, kLent, kRetired };
+    u64 *base = nullptr;
+    State state[kLaunchCursorSlots] = {};
+    unsigned long long owner[kLaunchCursorSlots] = {};  // stream id
+    cudaEvent_t done[kLaunchCursorSlots] = {};         // behind the owner's last launch
+};
+constexpr int kCursorPoolDevices = 64;
+std::mutex g_cursor_mutex;
+CursorPool g_cursor_pools[kCursorPoolDevices];
+
+// Runs launch(cursor) with a cursor lent to `stream`; launch zeroes it on the
+// stream before its kernel.  The lookup, the launch and an event recorded
+// behind it happen under one lock, so the launches that share a slot -- all
+// on its stream, hence in order -- each find it zeroed.  A slot passes to
+// another stream only once its event has completed.  A stream being captured
+// into a graph, or a launch that finds every slot busy, runs launch(nullptr):
+// the kernels' static grid-stride split, with the same results.
+template <class Launch>
+int with_stream_cursor(void *stream, Launch launch) {
+    using Pool = CursorPool;
+    const cudaStream_t s = as_stream(stream);
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    int dev = 0;
+    unsigned long long id = 0;
+    if (cudaStreamIsCapturing(s, &capture) != cudaSuccess || capture != cudaStreamCaptureStatusNone ||
+        cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kCursorPoolDevices ||
+        cudaStreamGetId(s, &id) != cudaSuccess) {
+        cudaGetLastError();
+        return launch(nullptr);
+    }
+    std::lock_guard<std::mutex> lock(g_cursor_mutex);
+    Pool &p = g_cursor_pools[dev];
+    if (!p.base) {
+        void *a = nullptr;
+        if (cudaGetSymbolAddress(&a, g_launch_cursors) != cudaSuccess) {
+            cudaGetLastError();
+            return launch(nullptr);
+        }
+        p.base = static_cast<u64 *>(a);
+    }
+    int slot = -1;
+    for (int i = 0; i < kLaunchCursorSlots && slot < 0; ++i)
+        if (p.state[i] == Pool::kLent && p.owner[i] == id) slot = i;
+    for (int i = 0; i < kLaunchCursorSlots && slot < 0; ++i) {
+        if (p.state[i] == Pool::kFree) {
+            if (cudaEventCreateWithFlags(&p.done[i], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                break;
+            }
+            slot = i;
+        } else if (p.state[i] == Pool::kLent && cudaEventQuery(p.done[i]) == cudaSuccess) {
+            slot = i;
+        }
+    }
+    if (cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();  // from the busy slots' queries
+    if (slot < 0) return launch(nullptr);
+    p.state[slot] = Pool::kLent;
+    p.owner[slot] = id;
+    const int rc = launch(p.base + (size_t)slot * kLaunchCursorStride);
+    // recorded whatever launch returned: its zeroing of the slot may be queued
+    if (cudaEventRecord(p.done[slot], s) != cudaSuccess) {
+        cudaGetLastError();
+        p.state[slot] = Pool::kRetired;  // its event no longer covers its work
+    }
+    return rc;
+}
+
+}  // namespace
+
 int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime, uint64_t *g_invert,
                  uint32_t *primecount, uint64_t capacity, uint32_t *overflow, void *stream, u64 *cursor);
 
@@ -175,7 +256,9 @@ int ww_launch_getsegprimes(uint64_t low, uint64_t high, int32_t wheelidx, uint64
                            uint64_t *g_invert, uint32_t *primecount, uint64_t capacity,
                            uint32_t *overflow, void *stream) {
     if (!g_prime || !g_invert) return set_err("null pointer"), WW_ERR_ARG;
-    return launch_sieve(low, high, wheelidx, g_prime, g_invert, primecount, capacity, overflow, stream, nullptr);
+    return with_stream_cursor(stream, [&](u64 *cursor) -> int {
+        return launch_sieve(low, high, wheelidx, g_prime, g_invert, primecount, capacity, overflow, stream, cursor);
+    });
 }
 
 }  // extern "C"
@@ -223,11 +306,14 @@ int ww_launch_wieferich(uint32_t *primecount, const uint64_t *g_prime, const uin
         !resultcount || !totalprimecount || !overflow)
         return set_err("null pointer"), WW_ERR_ARG;
     HitOut h{(u64 *)special_prime, rem, quot, result, resultcount, numresults, overflow};
-    k_wieferich<<<wieferich_grid(), kTestThreads, 0, as_stream(stream)>>>(
-        primecount, (const u64 *)g_prime, (const u64 *)g_invert, (u64 *)g_one, h, (u64 *)checksum,
-        (u64 *)totalprimecount, capacity, nullptr);
-    WW_CHECK_LAUNCH();
-    return WW_OK;
+    return with_stream_cursor(stream, [&](u64 *cursor) -> int {
+        if (cursor) WW_CU(cudaMemsetAsync(cursor, 0, sizeof(u64), as_stream(stream)));
+        k_wieferich<<<wieferich_grid(), kTestThreads, 0, as_stream(stream)>>>(
+            primecount, (const u64 *)g_prime, (const u64 *)g_invert, (u64 *)g_one, h, (u64 *)checksum,
+            (u64 *)totalprimecount, capacity, cursor);
+        WW_CHECK_LAUNCH();
+        return WW_OK;
+    });
 }
 
 int ww_launch_wallsunsun(const uint32_t *primecount, const uint64_t *g_prime,
@@ -239,11 +325,14 @@ int ww_launch_wallsunsun(const uint32_t *primecount, const uint64_t *g_prime,
         !resultcount || !overflow)
         return set_err("null pointer"), WW_ERR_ARG;
     HitOut h{(u64 *)special_prime, rem, quot, result, resultcount, numresults, overflow};
-    k_wallsunsun<<<wallsunsun_grid(), kTestThreads, 0, as_stream(stream)>>>(
-        primecount, (const u64 *)g_prime, (const u64 *)g_invert, (const u64 *)g_one, h,
-        (u64 *)checksum, capacity, nullptr);
-    WW_CHECK_LAUNCH();
-    return WW_OK;
+    return with_stream_cursor(stream, [&](u64 *cursor) -> int {
+        if (cursor) WW_CU(cudaMemsetAsync(cursor, 0, sizeof(u64), as_stream(stream)));
+        k_wallsunsun<<<wallsunsun_grid(), kTestThreads, 0, as_stream(stream)>>>(
+            primecount, (const u64 *)g_prime, (const u64 *)g_invert, (const u64 *)g_one, h,
+            (u64 *)checksum, capacity, cursor);
+        WW_CHECK_LAUNCH();
+        return WW_OK;
+    });
 }
 
 int ww_launch_test_prps(uint32_t *primecount, const uint64_t *g_prime, const uint64_t *g_invert,
@@ -254,11 +343,14 @@ int ww_launch_test_prps(uint32_t *primecount, const uint64_t *g_prime, const uin
         !resultcount || !totalprimecount || !overflow)
         return set_err("null pointer"), WW_ERR_ARG;
     HitOut h{(u64 *)special_prime, rem, quot, result, resultcount, numresults, overflow};
-    k_test_prps<<<test_grid(), kTestThreads, 0, as_stream(stream)>>>(
-        primecount, (const u64 *)g_prime, (const u64 *)g_invert, h, (u64 *)checksum,
-        (u64 *)totalprimecount, capacity, nullptr);
-    WW_CHECK_LAUNCH();
-    return WW_OK;
+    return with_stream_cursor(stream, [&](u64 *cursor) -> int {
+        if (cursor) WW_CU(cudaMemsetAsync(cursor, 0, sizeof(u64), as_stream(stream)));
+        k_test_prps<<<test_grid(), kTestThreads, 0, as_stream(stream)>>>(
+            primecount, (const u64 *)g_prime, (const u64 *)g_invert, h, (u64 *)checksum,
+            (u64 *)totalprimecount, capacity, cursor);
+        WW_CHECK_LAUNCH();
+        return WW_OK;
+    });
 }
 
 int ww_launch_digits(const uint64_t *primes, uint64_t n, uint64_t *out, void *stream) {
