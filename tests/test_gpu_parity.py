@@ -296,6 +296,23 @@ def test_bad_arguments_are_rejected(ww):
         assert c.counters()["seg_prp_count"] == 0
 
 
+def test_failed_reserve_leaves_context_usable(ww, ref_ranges):
+    """A PRP buffer that cannot be allocated leaves none: the reserve reports
+    WW_ERR_NOMEM, the sieve then refuses with WW_ERR_STATE, and a reserve
+    that fits makes the context run a range to the reference's result."""
+    r = ref_ranges["cross_2p32"]
+    with ww.Context(0, max_prps=1 << 18, max_hits=64) as c:
+        with pytest.raises(ww.WWError) as e:
+            c.reserve(1 << 40, 64)
+        assert e.value.status == -6
+        start, idx = ww.find_wheel_offset(r["lo"])
+        assert ww.lib().ww_sieve_prp(c.h, start, r["hi"], idx) == -8
+        c.reserve(1 << 18, 64)
+        got = c.run_range(r["lo"], r["hi"])
+        assert got["total_prp_count"] == r["prp_count"]
+        assert "%016X" % got["checksum"] == r["checksum"]
+
+
 def test_pipe_bench_runs(ww):
     for mode in range(6):
         ops, ms = ww.pipe_bench(mode)

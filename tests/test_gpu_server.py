@@ -111,3 +111,22 @@ def test_hit_overflow_is_reported_per_request(ww, ctx):
     for rid, a, b in reqs:
         ref = ctx.run_range(a, b)
         assert (done[rid]["checksum"], done[rid]["prp_count"]) == (ref["checksum"], ref["total_prp_count"])
+
+
+def test_failed_open_leaves_no_server(ww, ctx):
+    """A server whose PRP pool cannot be allocated is not left half open:
+    the open reports WW_ERR_NOMEM, a submit then finds no server, and a
+    server opened next on the same context serves a request to the plain
+    path's result."""
+    lo, hi = 10**12, 10**12 + 100_000
+    with pytest.raises(ww.WWError) as e:
+        ww.Server(ctx, prp_pool_bytes=1 << 50, max_active=4)
+    assert e.value.status == -6
+    req = (ww.Request * 1)(ww.Request(7, lo, hi))
+    assert ww.lib().ww_server_submit(ctx.h, req, 1) == -8
+    srv = ww.Server(ctx, prp_pool_bytes=1 << 26, max_active=4)
+    srv.submit([(7, lo, hi)])
+    (r,) = srv.drain()
+    srv.close()
+    ref = ctx.run_range(lo, hi)
+    assert (r["checksum"], r["prp_count"]) == (ref["checksum"], ref["total_prp_count"])

@@ -10,6 +10,7 @@
 #include <deque>
 #include <map>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <vector>
 
@@ -29,12 +30,15 @@ BatchState *&ctx_batch(ww_ctx *c);
 
 namespace {
 
+// A failed call leaves WW_ERR_NOMEM for an allocation, WW_ERR_CUDA otherwise,
+// and clears a non-sticky error so that the next launch check does not see it.
 #define WW_CU(call)                                                                             \
     do {                                                                                        \
         cudaError_t e_ = (call);                                                                \
         if (e_ != cudaSuccess) {                                                                \
             set_err("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
-            return WW_ERR_CUDA;                                                                 \
+            cudaGetLastError();                                                                 \
+            return e_ == cudaErrorMemoryAllocation ? WW_ERR_NOMEM : WW_ERR_CUDA;                \
         }                                                                                       \
     } while (0)
 
@@ -137,13 +141,12 @@ int ensure_capacity(BatchState &b, u32 n_units, u32 hit_cap) {
         WW_CU(cudaMallocHost(&b.h_first, ((size_t)n_units + 1) * sizeof(u64)));
         b.unit_cap = n_units;
     }
-    if (!b.d_next) {
-        WW_CU(cudaMalloc(&b.d_next, sizeof(u64)));
-        WW_CU(cudaMalloc(&b.d_rr, sizeof(u32)));
-        WW_CU(cudaMalloc(&b.d_epoch, sizeof(u32)));
-        WW_CU(cudaMalloc(&b.d_hit_count, sizeof(u32)));
-        WW_CU(cudaMalloc(&b.d_overflow, sizeof(u32)));
-    }
+    // each on its own, so a call after a failed one allocates what is missing
+    if (!b.d_next) WW_CU(cudaMalloc(&b.d_next, sizeof(u64)));
+    if (!b.d_rr) WW_CU(cudaMalloc(&b.d_rr, sizeof(u32)));
+    if (!b.d_epoch) WW_CU(cudaMalloc(&b.d_epoch, sizeof(u32)));
+    if (!b.d_hit_count) WW_CU(cudaMalloc(&b.d_hit_count, sizeof(u32)));
+    if (!b.d_overflow) WW_CU(cudaMalloc(&b.d_overflow, sizeof(u32)));
     if (hit_cap > b.hit_cap) {
         cudaFree(b.d_hit_unit);
         cudaFree(b.d_hit_p);
@@ -525,6 +528,8 @@ double mono_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+int server_init(ServerState &s, ww_ctx *ctx, const ww_server_cfg *cfg);
+
 }  // namespace
 
 extern "C" {
@@ -534,10 +539,25 @@ int ww_server_open(ww_ctx *ctx, const ww_server_cfg *cfg) {
         return set_err("bad server configuration"), WW_ERR_ARG;
     WW_CU(cudaSetDevice(ctx_device(ctx)));
     ServerState *&sv = ctx_server(ctx);
-    delete sv;
-    sv = new (std::nothrow) ServerState;
-    if (!sv) return set_err("host allocation failed"), WW_ERR_NOMEM;
-    ServerState &s = *sv;
+    if (sv) {
+        cudaStreamSynchronize((cudaStream_t)ctx_stream(ctx));
+        delete sv;
+        sv = nullptr;
+    }
+    // built aside and registered only when complete: a failed open leaves
+    // no server behind, and the destructor frees what was allocated
+    std::unique_ptr<ServerState> own(new (std::nothrow) ServerState);
+    if (!own) return set_err("host allocation failed"), WW_ERR_NOMEM;
+    const int rc = server_init(*own, ctx, cfg);
+    if (rc == WW_OK) sv = own.release();
+    return rc;
+}
+
+}  // extern "C"
+
+namespace {
+
+int server_init(ServerState &s, ww_ctx *ctx, const ww_server_cfg *cfg) {
     s.cfg = *cfg;
     ww_batch_cfg bc = default_cfg();
     if (BatchState *bs = ctx_batch(ctx)) bc = bs->cfg;  // the tuned configuration, if any
@@ -576,6 +596,10 @@ int ww_server_open(ww_ctx *ctx, const ww_server_cfg *cfg) {
     s.slots.assign(n, ServerSlot());
     return WW_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int ww_server_close(ww_ctx *ctx) {
     if (!ctx) return set_err("null ctx"), WW_ERR_ARG;

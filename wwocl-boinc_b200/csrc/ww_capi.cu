@@ -33,13 +33,16 @@ void set_err(const char *fmt, ...) {
 
 namespace {
 
-#define WW_CU(call)                                                                        \
-    do {                                                                                   \
-        cudaError_t e_ = (call);                                                           \
-        if (e_ != cudaSuccess) {                                                           \
+// A failed call leaves WW_ERR_NOMEM for an allocation, WW_ERR_CUDA otherwise,
+// and clears a non-sticky error so that the next launch check does not see it.
+#define WW_CU(call)                                                                             \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) {                                                                \
             set_err("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
-            return WW_ERR_CUDA;                                                            \
-        }                                                                                  \
+            cudaGetLastError();                                                                 \
+            return e_ == cudaErrorMemoryAllocation ? WW_ERR_NOMEM : WW_ERR_CUDA;                \
+        }                                                                                       \
     } while (0)
 
 #define WW_CHECK_LAUNCH() WW_CU(cudaGetLastError())
@@ -510,7 +513,14 @@ int ww_reserve(ww_ctx *c, uint64_t max_prps, uint32_t max_hits) {
             cudaMalloc(&c->hquot, (size_t)max_hits * 4) != cudaSuccess ||
             cudaMalloc(&c->hres, (size_t)max_hits * 4) != cudaSuccess) {
             cudaGetLastError();
-            return set_err("cannot allocate hit buffers"), WW_ERR_NOMEM;
+            // none or all: the launches check hprime alone
+            cudaFree(c->hprime);
+            cudaFree(c->hrem);
+            cudaFree(c->hquot);
+            cudaFree(c->hres);
+            c->hprime = nullptr;
+            c->hrem = c->hquot = c->hres = nullptr;
+            return set_err("cannot allocate hit buffers for %u entries", max_hits), WW_ERR_NOMEM;
         }
         c->hcap = max_hits;
     }
@@ -624,15 +634,14 @@ int ww_test_prps_host(ww_ctx *c, const uint64_t *host_primes, uint64_t n) {
     if (n == 0) return WW_OK;
     if (c->cap < 2) return set_err("PRP buffer too small for double buffering"), WW_ERR_ARG;
     WW_CU(cudaSetDevice(c->device));
-    if (!c->copy_stream) {
-        WW_CU(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
-        for (int i = 0; i < 2; ++i) {
-            WW_CU(cudaEventCreateWithFlags(&c->copied[i], cudaEventDisableTiming));
-            WW_CU(cudaEventCreateWithFlags(&c->consumed[i], cudaEventDisableTiming));
-        }
-        WW_CU(cudaMalloc(&c->d_chunk, 2 * kHostChunksMax * sizeof(u32)));
-        WW_CU(cudaMallocHost(&c->h_chunk, 2 * kHostChunksMax * sizeof(u32)));
+    // each resource on its own, so a call after a failed one creates what is missing
+    if (!c->copy_stream) WW_CU(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+        if (!c->copied[i]) WW_CU(cudaEventCreateWithFlags(&c->copied[i], cudaEventDisableTiming));
+        if (!c->consumed[i]) WW_CU(cudaEventCreateWithFlags(&c->consumed[i], cudaEventDisableTiming));
     }
+    if (!c->d_chunk) WW_CU(cudaMalloc(&c->d_chunk, 2 * kHostChunksMax * sizeof(u32)));
+    if (!c->h_chunk) WW_CU(cudaMallocHost(&c->h_chunk, 2 * kHostChunksMax * sizeof(u32)));
     // Chunks grow from 2^19 PRPs by doubling up to half the buffer, so the
     // one copy that nothing overlaps (the first) is short and every later
     // copy hides behind the test of the chunk before it.
