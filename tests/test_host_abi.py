@@ -228,3 +228,46 @@ def test_deep_table_rows_are_exact():
             q += 1
         if x > 1:
             assert pow(2, o // x, r) != 1, r
+
+
+def test_checkpoint_files_alternate_and_resume_from_newest(ww, tmp_path):
+    """write_state / read_state (main.cpp:103-209): the files alternate A, B,
+    A ...; the text is "start stop current cksm psum pcnt" with psum as %lf;
+    a read takes the valid file with the larger current (B on a tie) and
+    names the other file as the one to write next."""
+    fa, fb = str(tmp_path / "stateA-WW.txt"), str(tmp_path / "stateB-WW.txt")
+    start, stop = 10**12, 10**12 + 6 * 10**10
+    assert ww.state_read(fa, fb, start, stop) is None  # no files yet
+    nxt = True
+    for i, cur in enumerate((start + 10**10, start + 2 * 10**10, start + 3 * 10**10)):
+        nxt = ww.state_write(fa, fb, start, stop, cur, 0xABC0 + i, 1.5 * i, i, nxt)
+    # three writes: A, B, A -> B is due next
+    assert nxt is False
+    assert open(fa).read() == "%d %d %d %d %f %d\n" % (start, stop, start + 3 * 10**10, 0xABC2, 3.0, 2)
+    assert open(fb).read() == "%d %d %d %d %f %d\n" % (start, stop, start + 2 * 10**10, 0xABC1, 1.5, 1)
+    st, write_a = ww.state_read(fa, fb, start, stop)
+    assert st["current"] == start + 3 * 10**10 and st["cksm"] == 0xABC2 and st["pcnt"] == 2
+    assert write_a is False  # A was read, so B is overwritten next
+    # equal positions: B wins, A is written next
+    open(fb, "w").write(open(fa).read())
+    st, write_a = ww.state_read(fa, fb, start, stop)
+    assert write_a is True
+
+
+def test_checkpoint_files_that_do_not_belong_are_ignored(ww, tmp_path):
+    """A file that does not parse, or that was written for another start or
+    stop, is not used (main.cpp:147-175); the other file still is.  A
+    position outside [start, stop] is refused too (the reference would
+    resume from it)."""
+    fa, fb = str(tmp_path / "a.txt"), str(tmp_path / "b.txt")
+    start, stop = 10**9, 2 * 10**9
+    ww.state_write(fa, fb, start, stop, start + 5, 7, 0.0, 0, True)  # A
+    open(fb, "w").write("garbage\n")
+    st, write_a = ww.state_read(fa, fb, start, stop)
+    assert st["current"] == start + 5 and write_a is False
+    ww.state_write(fa, fb, start, stop + 1, start + 9, 8, 0.0, 0, False)  # B, for another range
+    st, _ = ww.state_read(fa, fb, start, stop)
+    assert st["current"] == start + 5
+    assert ww.state_read(fa, fb, start, stop + 1)[0]["current"] == start + 9
+    open(fa, "w").write("%d %d %d 0 0.000000 0\n" % (start, stop, stop + 1))  # past the end
+    assert ww.state_read(fa, fb, start, stop) is None
