@@ -167,6 +167,50 @@ WW_HD bool sprp2(u64 n, u64 &q_out) {
     return ok;
 }
 
+#if defined(__CUDACC__)
+// sprp2 for a whole warp: all 32 lanes call it, and lanes with act false test
+// the first active lane's number and return false.  The squarings above
+// every lane's bit t touch neither the value at bit t nor the -1 check, so
+// they run in a first loop without that bookkeeping; the second loop is
+// sprp2's own, from the warp's largest t down.
+__device__ __forceinline__ bool sprp2_warp(u64 n, bool act, u64 &q_out) {
+    const u32 live = __ballot_sync(0xffffffffu, act);
+    if (live == 0) {
+        q_out = 0;
+        return false;
+    }
+    const u64 src = __shfl_sync(0xffffffffu, n, __ffs((int)live) - 1);
+    n = act ? n : src;
+    const u64 q = inv64(n);
+    q_out = q;
+    const u64 one = r_mod(n);
+    const u64 mone = n - one;
+    const u64 nm1 = n - 1;
+    const int t = __ffsll((long long)nm1) - 1;  // >= 1: n is odd
+    const int top = 63 - __clzll((long long)nm1);
+    const int tw = (int)__reduce_max_sync(0xffffffffu, (unsigned)t);
+    u64 a = add_mod(one, one, n);
+    int i = top - 1;
+    for (; i > tw; --i) {
+        a = mont_mul(a, a, n, q);
+        const u64 d = add_mod(a, a, n);
+        a = ((nm1 >> i) & 1) ? d : a;
+    }
+    u64 at_t = 0;
+    bool m1 = false;
+    for (; i >= 1; --i) {
+        a = mont_mul(a, a, n, q);
+        const u64 d = add_mod(a, a, n);
+        a = ((nm1 >> i) & 1) ? d : a;
+        at_t = (i == t) ? a : at_t;
+        m1 |= (i < t) & (a == mone);
+    }
+    const bool ok = (at_t == one) | (at_t == mone) | m1;
+    return act && ok;
+}
+#endif
+
+// ----------------------------------------------------------------- mod p^2
 // ----------------------------------------------------------------- mod p^2
 
 struct ModP2 {

@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(Cfg::kThreads) k_tiles(BatchArgs a) {
         auto sprp_step = [&](u32 j, bool act) {
             const u64 n = nbase + 2ull * j;
             u64 q = 0;
-            const bool pass = act && prp_test(n, q);
+            const bool pass = prp_test_warp(n, act, q);
             const u32 ballot = __ballot_sync(0xffffffffu, pass);
             const u32 rank = __popc(ballot & ((1u << lane) - 1u));
             if (pass) pq[pn + rank] = n;

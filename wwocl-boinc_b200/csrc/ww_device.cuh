@@ -140,7 +140,7 @@ struct PrpOut {
 
 __device__ __forceinline__ void sprp_emit(const PrpOut &out, u64 n, bool active) {
     u64 q = 0;
-    const bool pass = active && prp_test(n, q);
+    const bool pass = prp_test_warp(n, active, q);
     const u32 ballot = __ballot_sync(0xffffffffu, pass);
     if (ballot == 0) return;
     const int lane = threadIdx.x & 31;

@@ -49,6 +49,17 @@ typedef Arith64 WW_ARITH;
 WW_HD bool prp_test(u64 n, u64 &q) { return sprp2(n, q); }
 #endif
 
+#if defined(__CUDACC__)
+// prp_test for a whole warp (all lanes call it; act false gives false)
+__device__ __forceinline__ bool prp_test_warp(u64 n, bool act, u64 &q) {
+#if defined(WW_ARITH_VERSION) && WW_ARITH_VERSION == 2
+    return act && sprp2_32(n, q);
+#else
+    return sprp2_warp(n, act, q);
+#endif
+}
+#endif
+
 WW_HD int top_bit(u64 x) {
 #if defined(__CUDA_ARCH__)
     return 63 - __clzll((long long)x);
