@@ -313,6 +313,32 @@ def test_failed_reserve_leaves_context_usable(ww, ref_ranges):
         assert "%016X" % got["checksum"] == r["checksum"]
 
 
+def test_sync_and_marker_time_out_then_complete(ww):
+    """ww_sync and ww_wait_marker give up with WW_ERR_TIMEOUT while work is
+    still running (main.cpp:329-446 poll the same way), the context stays
+    usable, and a later wait completes: the counters then hold three passes
+    of the tests over one sieved list."""
+    lo = 2**64 - 2**35
+    hi = lo + 2**32
+    L = ww.lib()
+    with ww.Context(0, max_prps=1 << 27, max_hits=64) as c:
+        one = c.run_range(lo, hi)
+        c.clear_results()
+        c.clear_segment()
+        c.sieve_prp(lo, hi)
+        for _ in range(3):  # about 0.3 s of queued work
+            c.test_prps()
+        c.marker(0)
+        assert L.ww_wait_marker(c.h, 0, 1) == -5
+        assert L.ww_sync(c.h, 1) == -5
+        c.sync()
+        assert L.ww_wait_marker(c.h, 0, 1) == 0
+        k = c.counters()
+        assert k["overflow"] == 0
+        assert k["total_prp_count"] == 3 * one["total_prp_count"]
+        assert k["checksum"] == (3 * one["checksum"]) % 2**64
+
+
 def test_pipe_bench_runs(ww):
     for mode in range(6):
         ops, ms = ww.pipe_bench(mode)
