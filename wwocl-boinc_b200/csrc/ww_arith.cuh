@@ -190,18 +190,21 @@ __device__ __forceinline__ bool sprp2_warp(u64 n, bool act, u64 &q_out) {
     const int top = 63 - __clzll((long long)nm1);
     const int tw = (int)__reduce_max_sync(0xffffffffu, (unsigned)t);
     u64 a = add_mod(one, one, n);
+    u64 ebits = nm1 << (64 - top);  // bit top-1 of n-1 at bit 63
     int i = top - 1;
     for (; i > tw; --i) {
         a = mont_mul(a, a, n, q);
         const u64 d = add_mod(a, a, n);
-        a = ((nm1 >> i) & 1) ? d : a;
+        a = ((long long)ebits < 0) ? d : a;
+        ebits <<= 1;
     }
     u64 at_t = 0;
     bool m1 = false;
     for (; i >= 1; --i) {
         a = mont_mul(a, a, n, q);
         const u64 d = add_mod(a, a, n);
-        a = ((nm1 >> i) & 1) ? d : a;
+        a = ((long long)ebits < 0) ? d : a;
+        ebits <<= 1;
         at_t = (i == t) ? a : at_t;
         m1 |= (i < t) & (a == mone);
     }
