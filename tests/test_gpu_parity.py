@@ -266,6 +266,41 @@ def test_kernel_shaped_launchers_on_many_streams(ww, ref_ranges):
             cudart.cudaStreamDestroy(h)
 
 
+def test_kernel_shaped_launchers_from_host_threads(ww, ref_ranges):
+    """Four host threads, each with its own stream and buffers, queue the
+    reference kernel sequence five times each at the same time (the foreign
+    calls release the interpreter lock): every stream's results equal the
+    reference's."""
+    import threading
+
+    import torch
+
+    dev = torch.device("cuda", 0)
+    names = ["cross_2p32", "wieferich_special_window", "near_top_2e6", "wss_special_window"]
+    streams = [torch.cuda.Stream(dev, priority=-1 if i % 2 else 0) for i in range(4)]
+    seqs = [_KernelSequence(ww, ref_ranges[n], cap=1 << 17, nres=64) for n in names]
+    torch.cuda.synchronize(dev)
+    errors = []
+
+    def work(k):
+        try:
+            torch.cuda.set_device(dev)
+            for _ in range(5):
+                seqs[k].launch(streams[k].cuda_stream)
+        except Exception as e:  # noqa: BLE001 -- reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=work, args=(k,)) for k in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    torch.cuda.synchronize(dev)
+    assert not errors, errors
+    for k, q in enumerate(seqs):
+        q.check("thread %d" % k)
+
+
 def test_kernel_shaped_launchers_under_graph_capture(ww, ref_ranges):
     """Launches captured into a CUDA graph (no cursor there) replay to the
     reference's results, twice."""
