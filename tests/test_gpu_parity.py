@@ -171,6 +171,45 @@ def test_prp_overflow_is_reported(ww, oracle):
         assert e.value.status == -3
 
 
+@pytest.mark.parametrize("slack", [0, -1])
+def test_prp_buffer_exact_fit(ww, ref_prps, slack):
+    """A PRP buffer of exactly the range's PRP count holds the whole list
+    (the reference's set); one entry less sets the overflow flag, still
+    counts every PRP, and keeps the list unreadable (the reference's
+    check is count > mem_size, main.cpp:801-805)."""
+    r = ref_prps["prp_top"]
+    with ww.Context(0, max_prps=r["count"] + slack, max_hits=16) as c:
+        c.clear_results()
+        c.clear_segment()
+        c.sieve_prp(r["lo"], r["hi"])
+        c.sync()
+        k = c.counters()
+        assert k["seg_prp_count"] == r["count"]
+        if slack == 0:
+            assert k["overflow"] == 0
+            assert _digest(c.prps()) == (r["count"], r["sum_mod_2_64"], r["sha256"])
+        else:
+            assert k["overflow"] & 1
+            with pytest.raises(ww.WWError) as e:
+                c.prps()
+            assert e.value.status == -3
+
+
+def test_hit_buffer_exact_fit(ww, ref_ranges):
+    """A hit buffer of exactly the range's hit count keeps every hit with
+    no overflow flag; one less overflows (the reference's check is
+    count > numresults, main.cpp:811-814)."""
+    r = ref_ranges["small_3e6"]
+    for cap, over in ((r["cpu_results"], False), (r["cpu_results"] - 1, True)):
+        with ww.Context(0, max_prps=1 << 19, max_hits=cap) as c:
+            got = c.run_range(r["lo"], r["hi"])
+            assert got["result_count"] == r["cpu_results"]
+            assert "%016X" % got["checksum"] == r["checksum"]
+            assert bool(got["overflow"] & 2) == over
+            if not over:
+                assert len(got["hits"]) == r["cpu_results"]
+
+
 def test_hit_overflow_is_reported(ww):
     with ww.Context(0, max_prps=1 << 20, max_hits=10) as c:
         got = c.run_range(127, 1_000_000)
