@@ -253,6 +253,9 @@ int ww_batch_tune(ww_ctx *ctx, const ww_unit *sample, uint32_t n, ww_batch_cfg *
  * each clears it, and calls whose GPU work overlaps race, so keep them on
  * one stream.  The first call on a device sets up the array's address
  * (cudaGetSymbolAddress) and should come before any stream capture.
+ * *hit_count receives the number of hits found.  When that exceeds
+ * min(hit_cap, 4096), the records hold that many of them, in no set
+ * order, and out[i].hits still counts every hit of range i.
  * Returns WW_ERR_ARG for more than 4096 ranges. */
 int ww_batch_run_noalloc(const ww_unit *units, uint32_t n, ww_unit_result *out, ww_hit *hits,
                          uint32_t *hit_unit, uint32_t hit_cap, uint32_t *hit_count, void *stream);

@@ -58,6 +58,28 @@ def test_noalloc_matches_batch_twice(ww):
         assert nh == len(want_hits) and hits == want_hits
 
 
+@pytest.mark.parametrize("hit_cap", [100, 4096])
+def test_noalloc_reports_more_hits_than_records(ww, ref_ranges, hit_cap):
+    """Two overlapping copies of [127, 5e7) find 2 x 3890 hits: more than
+    the caller's records (100) or the scratch's (4096).  *hit_count still
+    gives the total, each range its own count and the reference's
+    checksum, and every record kept is one of the hits that ww_batch_run
+    finds."""
+    r = ref_ranges["config1_5e7"]
+    units = [(r["lo"], r["hi"]), (r["lo"], r["hi"])]
+    with ww.Context(0, max_prps=1 << 20, max_hits=15000) as ctx:
+        b = ww.Batch(ctx)
+        b.set_config(8192, 256, 1)
+        b.run(units)
+        want_hits = set(b.hits())
+    got, hits, nh = _noalloc(ww, units, hit_cap=hit_cap)
+    assert nh == 2 * r["cpu_results"]
+    for checksum, prp_count, unit_hits in got:
+        assert "%016X" % checksum == r["checksum"]
+        assert prp_count == r["prp_count"] and unit_hits == r["cpu_results"]
+    assert len(hits) == hit_cap and set(hits) <= want_hits
+
+
 def test_noalloc_rejects_too_many_ranges(ww):
     L = ww.lib()
     n = 4097
