@@ -58,6 +58,40 @@ def test_two_rank_split_sums_to_reference(ww, ctx):
     assert "%016X" % (total_c % 2**64) == LONG["checksum"]
 
 
+def test_kernel_shaped_loop_matches_reference(ww):
+    """The reference program's own loop (main.cpp:1683-1795) through the
+    drop-in launchers on caller-owned memory: clearresult once, then per
+    2^30-number segment clearn, getsegprimes, wieferich, wallsunsun."""
+    import torch
+
+    L = ww.lib()
+    dev = torch.device("cuda", 0)
+    cap, nres = 1 << 25, 15000
+    e = lambda n, dt: torch.empty(n, dtype=dt, device=dev)  # noqa: E731
+    prime, inv, one = e(cap, torch.int64), e(cap, torch.int64), e(2 * cap, torch.int64)
+    sp, rem, quot, res = e(nres, torch.int64), e(nres, torch.int32), e(nres, torch.int32), e(nres, torch.int32)
+    cks, total, rc, pc = e(1, torch.int64), e(1, torch.int64), e(1, torch.int32), e(2, torch.int32)
+    ovf = torch.zeros(1, dtype=torch.int32, device=dev)
+    s = torch.cuda.Stream(dev)
+    st = s.cuda_stream
+    P = lambda t: t.data_ptr()  # noqa: E731
+    torch.cuda.synchronize(dev)
+    ww.check(L.ww_launch_clearresult(P(cks), P(rc), P(total), P(pc), st), "clearresult")
+    for a, b in _units(1 << 30):
+        start, idx = ww.find_wheel_offset(a)
+        ww.check(L.ww_launch_clearn(P(pc), st), "clearn")
+        ww.check(L.ww_launch_getsegprimes(start, b, idx, P(prime), P(inv), P(pc), cap, P(ovf), st), "gsp")
+        ww.check(L.ww_launch_wieferich(P(pc), P(prime), P(inv), P(one), P(sp), P(rem), P(quot), P(res), P(cks),
+                                       P(rc), P(total), cap, nres, P(ovf), st), "wieferich")
+        ww.check(L.ww_launch_wallsunsun(P(pc), P(prime), P(inv), P(one), P(sp), P(rem), P(quot), P(res), P(cks),
+                                        P(rc), cap, nres, P(ovf), st), "wallsunsun")
+    s.synchronize()
+    assert int(ovf.item()) == 0
+    assert int(total.item()) == LONG["prp_count"]
+    assert "%016X" % (int(cks.item()) % 2**64) == LONG["checksum"]
+    assert int(rc.item()) == LONG["cpu_results"]
+
+
 @pytest.mark.parametrize("case", [1, 2, 3])
 def test_shard_entry_writes_reference_results(tests_txt, tmp_path, case):
     """shard.py's entry point (what torchrun starts on each GPU) on the
