@@ -25,8 +25,9 @@ namespace ww {
 // Sieve + SPRP over [lo, hi).  b0 = lo & ~1; segment s holds the odd numbers
 // b0 + 2(s*kSegOdd + j) + 1, j < kSegOdd.
 // With a segment cursor (zeroed before the launch) the CTAs take segments
-// one at a time from it; without one (the kernel-shaped entry point) they
-// stride over the segments.
+// one at a time from it; without one (a launch captured into a graph, or
+// one that found every cursor of the library's pool busy) they stride over
+// the segments.
 __global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out, u64 *cursor,
                                                              const DeepRow *deep) {
     __shared__ u32 bitmap[kSegWords];
@@ -146,8 +147,9 @@ constexpr u64 kWarpFetch = 32;
 
 // Runs f(i) for every list index i < n.  With a work cursor (zeroed before
 // the launch) each warp pulls kWarpFetch indices at a time, so warps that run
-// ahead take more of the list and all finish together; without one (the
-// kernel-shaped entry points, which have no scratch) the grid strides.
+// ahead take more of the list and all finish together; without one (a
+// launch captured into a graph, or one that found every cursor of the
+// library's pool busy) the grid strides.
 template <class F>
 __device__ __forceinline__ void for_each_prime(u64 n, u64 *cursor, F &&f) {
     if (cursor) {
