@@ -236,7 +236,7 @@ class _KernelSequence:
         self.rc, self.pc, self.ovf = e(1, torch.int32), e(2, torch.int32), torch.zeros(1, dtype=torch.int32,
                                                                                          device=dev)
 
-    def launch(self, st):
+    def launch(self, st, fused=False):
         ww, L, r, cap, nres = self.ww, self.L, self.r, self.cap, self.nres
         P = lambda t: t.data_ptr()  # noqa: E731
         start, idx = ww.find_wheel_offset(r["lo"])
@@ -244,6 +244,11 @@ class _KernelSequence:
         ww.check(L.ww_launch_clearn(P(self.pc), st), "clearn")
         ww.check(L.ww_launch_getsegprimes(start, r["hi"], idx, P(self.prime), P(self.inv), P(self.pc), cap,
                                           P(self.ovf), st), "gsp")
+        if fused:  # both tests in one launch
+            ww.check(L.ww_launch_test_prps(P(self.pc), P(self.prime), P(self.inv), P(self.sp), P(self.rem),
+                                           P(self.quot), P(self.res), P(self.cks), P(self.rc), P(self.total), cap,
+                                           nres, P(self.ovf), st), "test_prps")
+            return
         ww.check(L.ww_launch_wieferich(P(self.pc), P(self.prime), P(self.inv), P(self.one), P(self.sp), P(self.rem),
                                        P(self.quot), P(self.res), P(self.cks), P(self.rc), P(self.total), cap, nres,
                                        P(self.ovf), st), "wieferich")
@@ -268,6 +273,19 @@ def test_kernel_shaped_launchers_on_torch_memory(ww, ref_ranges):
     seq.launch(s.cuda_stream)
     s.synchronize()
     seq.check()
+
+
+@pytest.mark.parametrize("name", ["small_3e6", "wieferich_special_window", "wss_special_window", "cross_2p63"])
+def test_fused_kernel_shaped_launcher(ww, ref_ranges, name):
+    """ww_launch_test_prps in place of the wieferich + wallsunsun pair: the
+    same checksum, counts and hit records as the reference."""
+    import torch
+
+    seq = _KernelSequence(ww, ref_ranges[name], cap=1 << 18, nres=15000)
+    s = torch.cuda.Stream(torch.device("cuda", 0))
+    seq.launch(s.cuda_stream, fused=True)
+    s.synchronize()
+    seq.check(name)
 
 
 def test_kernel_shaped_launchers_on_many_streams(ww, ref_ranges):

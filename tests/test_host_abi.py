@@ -271,3 +271,11 @@ def test_checkpoint_files_that_do_not_belong_are_ignored(ww, tmp_path):
     assert ww.state_read(fa, fb, start, stop + 1)[0]["current"] == start + 9
     open(fa, "w").write("%d %d %d 0 0.000000 0\n" % (start, stop, stop + 1))  # past the end
     assert ww.state_read(fa, fb, start, stop) is None
+
+
+def test_status_strings(ww):
+    """Every status code of the header has its own message."""
+    L = ww.lib()
+    seen = {code: L.ww_status_string(code).decode() for code in range(-9, 1)}
+    assert seen[0] == "ok" and len(set(seen.values())) == len(seen)
+    assert L.ww_status_string(-100).decode() == "unknown status"
