@@ -375,6 +375,40 @@ def test_kernel_shaped_launchers_under_graph_capture(ww, ref_ranges):
         seq.check()
 
 
+def test_context_buffers_drive_the_kernel_shaped_launchers(ww, ref_ranges):
+    """ww_get_buffers hands out the context's own device buffers and stream:
+    the kernel-shaped sequence run on them leaves counters and hits that
+    the context's read-backs return, equal to the reference's."""
+    r = ref_ranges["wss_special_window"]
+    L = ww.lib()
+    with ww.Context(0, max_prps=1 << 18, max_hits=64) as c:
+        b = c.buffers()
+        assert b.prp_capacity == 1 << 18 and b.hit_capacity == 64
+        start, idx = ww.find_wheel_offset(r["lo"])
+        ww.check(L.ww_launch_clearresult(b.checksum, b.result_count, b.total_prp_count, b.primecount, b.stream),
+                 "clearresult")
+        ww.check(L.ww_launch_clearn(b.primecount, b.stream), "clearn")
+        ww.check(L.ww_launch_getsegprimes(start, r["hi"], idx, b.prime, b.invert, b.primecount, b.prp_capacity,
+                                          b.overflow, b.stream), "gsp")
+        ww.check(L.ww_launch_wieferich(b.primecount, b.prime, b.invert, b.one, b.special_prime, b.rem, b.quot,
+                                       b.result, b.checksum, b.result_count, b.total_prp_count, b.prp_capacity,
+                                       b.hit_capacity, b.overflow, b.stream), "wieferich")
+        ww.check(L.ww_launch_wallsunsun(b.primecount, b.prime, b.invert, b.one, b.special_prime, b.rem, b.quot,
+                                        b.result, b.checksum, b.result_count, b.prp_capacity, b.hit_capacity,
+                                        b.overflow, b.stream), "wallsunsun")
+        c.sync()
+        k = c.counters()
+        assert k["overflow"] == 0 and k["total_prp_count"] == r["prp_count"]
+        assert "%016X" % k["checksum"] == r["checksum"]
+        assert k["result_count"] == r["cpu_results"] == len(c.hits())
+        assert sorted(c.hits()) == sorted(_range_hits(ww, r))
+
+
+def _range_hits(ww, r):
+    with ww.Context(0, max_prps=1 << 18, max_hits=64) as c:
+        return c.run_range(r["lo"], r["hi"])["hits"]
+
+
 def test_bad_arguments_are_rejected(ww):
     with ww.Context(0, max_prps=1024, max_hits=16) as c:
         L = ww.lib()
