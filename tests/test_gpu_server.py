@@ -3,6 +3,8 @@
 admission respects the PRP-buffer memory budget."""
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -130,3 +132,26 @@ def test_failed_open_leaves_no_server(ww, ctx):
     srv.close()
     ref = ctx.run_range(lo, hi)
     assert (r["checksum"], r["prp_count"]) == (ref["checksum"], ref["total_prp_count"])
+
+
+def test_calls_out_of_order_are_refused(ww, ctx):
+    """Without an open server every call reports WW_ERR_STATE; closing is
+    idempotent; an empty submit is a no-op; a request's PRP list can be
+    asked for once it is done, and not before or for an unknown id."""
+    L = ww.lib()
+    n = C.c_uint32(0)
+    q, a, u = C.c_uint32(0), C.c_uint32(0), C.c_uint64(0)
+    assert L.ww_server_close(ctx.h) == 0
+    assert L.ww_server_step(ctx.h, None, 0, C.byref(n)) == -8
+    assert L.ww_server_status(ctx.h, C.byref(q), C.byref(a), C.byref(u)) == -8
+    assert L.ww_server_hits(ctx.h, 1, None, 0, C.byref(n)) == -8
+    assert L.ww_server_close(ctx.h) == 0
+    srv = ww.Server(ctx, prp_pool_bytes=1 << 26, max_active=4)
+    srv.submit([])
+    assert srv.status() == (0, 0, 0)
+    assert L.ww_server_prps(ctx.h, 42, None, 0, C.byref(u)) == -8  # no such request
+    srv.submit([(42, 10**12, 10**12 + 200_000)])
+    (r,) = srv.drain()
+    assert r["id"] == 42 and len(srv.prps(42, r["prps_stored"])) == r["prp_count"]
+    srv.close()
+    srv.close()
