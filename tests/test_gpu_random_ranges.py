@@ -13,7 +13,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _ranges(seed=2026, n=40):
+def _ranges(seed=2026, n=200):
     rng = random.Random(seed)
     out = []
     for _ in range(n):
