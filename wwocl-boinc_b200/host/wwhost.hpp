@@ -13,6 +13,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <thread>
 #include <chrono>
 #include <string>
 #include <vector>
@@ -87,20 +88,48 @@ inline bool truncate_results(const Files &f) {
 // The primes of [lo, hi) for lo >= 127, the list primesieve produced in the
 // reference's PRP check (main.cpp:498): numbers with no prime factor <= 113
 // that pass the deterministic Miller-Rabin test.
+// Splits [lo, hi) into contiguous pieces, one per host thread (at most 16,
+// none shorter than 2^16 numbers), and runs f(a, b, i) on piece i = [a, b)
+// in its own thread.  Returns the number of pieces.
+template <class F>
+inline unsigned parallel_pieces(uint64_t lo, uint64_t hi, F f) {
+    if (hi <= lo) return 0;
+    unsigned t = std::thread::hardware_concurrency();
+    t = t < 1 ? 1 : (t > 16 ? 16 : t);
+    const uint64_t span = hi - lo;
+    const uint64_t by_size = span / 65536 + 1;
+    const unsigned parts = (unsigned)(by_size < t ? by_size : t);
+    std::vector<std::thread> pool;
+    for (unsigned i = 0; i < parts; ++i) {
+        const uint64_t a = lo + span / parts * i;
+        const uint64_t b = i + 1 == parts ? hi : lo + span / parts * (i + 1);
+        pool.emplace_back([=, &f] { f(a, b, i); });
+    }
+    for (std::thread &th : pool) th.join();
+    return parts;
+}
+
+// The primes of [lo, hi) with no factor up to 113 (the CPU side of
+// checkPRPS, main.cpp:451-523), in increasing order; the pieces of the
+// range are tested on all host threads.
 inline std::vector<uint64_t> cpu_primes(uint64_t lo, uint64_t hi) {
     static const uint32_t small[29] = {3,  5,  7,  11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53,
                                        59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113};
+    std::vector<std::vector<uint64_t>> part(16);
+    const unsigned parts = parallel_pieces(lo, hi, [&](uint64_t a, uint64_t b, unsigned i) {
+        for (uint64_t n = a | 1; n < b && n >= a; n += 2) {
+            bool sf = false;
+            for (uint32_t r : small)
+                if (n % r == 0) {
+                    sf = true;
+                    break;
+                }
+            if (!sf && ww_is_prime(n)) part[i].push_back(n);
+            if (n > UINT64_MAX - 2) break;
+        }
+    });
     std::vector<uint64_t> out;
-    for (uint64_t n = lo | 1; n < hi && n >= lo; n += 2) {
-        bool sf = false;
-        for (uint32_t r : small)
-            if (n % r == 0) {
-                sf = true;
-                break;
-            }
-        if (!sf && ww_is_prime(n)) out.push_back(n);
-        if (n > UINT64_MAX - 2) break;
-    }
+    for (unsigned i = 0; i < parts; ++i) out.insert(out.end(), part[i].begin(), part[i].end());
     return out;
 }
 

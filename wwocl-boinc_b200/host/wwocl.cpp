@@ -216,9 +216,22 @@ void self_test(ww_ctx *ctx, uint64_t start, uint64_t top, uint64_t calc_range, u
     if (debug) printf("Verifying GPU kernels using range %" PRIu64 " to %" PRIu64 "...\n", start, stop);
     must(ww_clear_results(ctx), "clearresult");
     enqueue_segment(ctx, start, stop, separate);
+    // the host twin on every host thread while the GPU works; the sums do
+    // not depend on how the range is split
     uint64_t prp = 0, cks = 0;
     uint32_t res = 0;
-    must(ww_selftest_range(start, stop, &prp, &cks, &res), "host self-test");
+    uint64_t part_prp[16] = {}, part_cks[16] = {};
+    uint32_t part_res[16] = {};
+    int part_rc[16] = {};
+    const unsigned parts = parallel_pieces(start, stop, [&](uint64_t a, uint64_t b, unsigned i) {
+        part_rc[i] = ww_selftest_range(a, b, &part_prp[i], &part_cks[i], &part_res[i]);
+    });
+    for (unsigned i = 0; i < parts; ++i) {
+        must(part_rc[i], "host self-test");
+        prp += part_prp[i];
+        cks += part_cks[i];
+        res += part_res[i];
+    }
     must(ww_sync(ctx, 600000), "sync");
     const uint32_t gpuprimecount = check_prps(ctx, start, stop, cap);
     if (gpuprimecount != prp) {
