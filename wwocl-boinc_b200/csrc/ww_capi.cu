@@ -283,17 +283,22 @@ int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prim
     const uint64_t span = high - b0;
     const uint64_t per = 2ull * kSegOdd;
     const uint64_t nseg = span / per + (span % per ? 1 : 0);
+    WW_CU(cudaFuncSetAttribute(k_sieve_prp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSieveSmem));
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sieve_prp, kSieveThreads, 0) != cudaSuccess ||
-        per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sieve_prp, kSieveThreads, kSieveSmem) !=
+            cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
         per_sm = 1;
+    }
     const uint64_t slots = (uint64_t)sm_count() * (uint64_t)per_sm;
     const uint64_t grid = nseg < slots ? nseg : slots;
     PrpOut out{(u64 *)g_prime, (u64 *)g_invert, primecount, capacity, overflow};
     const DeepRow *deep = deep_rows_device();
     if (!deep) return WW_ERR_CUDA;
     if (cursor) WW_CU(cudaMemsetAsync(cursor, 0, sizeof(u64), as_stream(stream)));
-    k_sieve_prp<<<(unsigned)grid, kSieveThreads, 0, as_stream(stream)>>>(low, high, nseg, out, cursor, deep);
+    k_sieve_prp<<<(unsigned)grid, kSieveThreads, kSieveSmem, as_stream(stream)>>>(low, high, nseg, out, cursor,
+                                                                                   deep);
     WW_CHECK_LAUNCH();
     return WW_OK;
 }

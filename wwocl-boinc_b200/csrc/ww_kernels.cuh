@@ -28,10 +28,12 @@ namespace ww {
 // one at a time from it; without one (a launch captured into a graph, or
 // one that found every cursor of the library's pool busy) they stride over
 // the segments.
-__global__ void __launch_bounds__(kSieveThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out, u64 *cursor,
-                                                             const DeepRow *deep) {
-    __shared__ u32 bitmap[kSegWords];
-    __shared__ u32 queue[kSieveWarps][kQueueCap];
+__global__ void __launch_bounds__(kSieveThreads, 2048 / kSieveThreads / 2) k_sieve_prp(u64 lo, u64 hi, u64 nseg,
+                                                                                       PrpOut out, u64 *cursor,
+                                                                                       const DeepRow *deep) {
+    extern __shared__ u32 sieve_smem[];  // kSieveSmem bytes
+    u32 *bitmap = sieve_smem;
+    u32(*queue)[kQueueCap] = reinterpret_cast<u32(*)[kQueueCap]>(sieve_smem + kSegWords);
     __shared__ u32 s_chunk;
     __shared__ u64 s_seg;
     const u64 b0 = lo & ~1ull;
