@@ -266,6 +266,37 @@ int ww_launch_getsegprimes(uint64_t low, uint64_t high, int32_t wheelidx, uint64
 
 }  // extern "C"
 
+namespace {
+
+// Resident CTAs of k_sieve_prp<G> on the current device (the dynamic
+// shared memory limit is raised first).
+template <class G>
+cudaError_t sieve_slots(int *slots) {
+    cudaError_t e = cudaFuncSetAttribute(k_sieve_prp<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::kSmem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sieve_prp<G>, G::kThreads, G::kSmem);
+    if (e != cudaSuccess) return e;
+    *slots = sm_count() * (per_sm < 1 ? 1 : per_sm);
+    return cudaSuccess;
+}
+
+template <class G>
+int launch_sieve_shape(uint64_t low, uint64_t high, uint64_t span, const PrpOut &out, u64 *cursor,
+                       const DeepRow *deep, cudaStream_t stream) {
+    const uint64_t per = 2ull * G::kOdd;
+    const uint64_t nseg = span / per + (span % per ? 1 : 0);
+    int slots = 0;
+    WW_CU(sieve_slots<G>(&slots));
+    const uint64_t grid = nseg < (uint64_t)slots ? nseg : (uint64_t)slots;
+    if (cursor) WW_CU(cudaMemsetAsync(cursor, 0, sizeof(u64), stream));
+    k_sieve_prp<G><<<(unsigned)grid, G::kThreads, G::kSmem, stream>>>(low, high, nseg, out, cursor, deep);
+    WW_CHECK_LAUNCH();
+    return WW_OK;
+}
+
+}  // namespace
+
 // The sieve launch; with a segment cursor (zeroed here, on the stream) the
 // CTAs take segments dynamically instead of striding.
 int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime, uint64_t *g_invert,
@@ -281,26 +312,17 @@ int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prim
         return set_err("range too wide for a 32-bit PRP counter"), WW_ERR_ARG;
     const uint64_t b0 = low & ~1ull;
     const uint64_t span = high - b0;
-    const uint64_t per = 2ull * kSegOdd;
-    const uint64_t nseg = span / per + (span % per ? 1 : 0);
-    WW_CU(cudaFuncSetAttribute(k_sieve_prp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSieveSmem));
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sieve_prp, kSieveThreads, kSieveSmem) !=
-            cudaSuccess ||
-        per_sm < 1) {
-        cudaGetLastError();
-        per_sm = 1;
-    }
-    const uint64_t slots = (uint64_t)sm_count() * (uint64_t)per_sm;
-    const uint64_t grid = nseg < slots ? nseg : slots;
     PrpOut out{(u64 *)g_prime, (u64 *)g_invert, primecount, capacity, overflow};
     const DeepRow *deep = deep_rows_device();
     if (!deep) return WW_ERR_CUDA;
-    if (cursor) WW_CU(cudaMemsetAsync(cursor, 0, sizeof(u64), as_stream(stream)));
-    k_sieve_prp<<<(unsigned)grid, kSieveThreads, kSieveSmem, as_stream(stream)>>>(low, high, nseg, out, cursor,
-                                                                                   deep);
-    WW_CHECK_LAUNCH();
-    return WW_OK;
+    // the wide shape once the range gives each of its resident CTAs a
+    // segment; below that the narrow one, which has twice the segments
+    int wide_slots = 0;
+    WW_CU(sieve_slots<SieveWide>(&wide_slots));
+    const uint64_t wide_segs = span / (2ull * SieveWide::kOdd) + 1;
+    if (wide_segs >= (uint64_t)wide_slots)
+        return launch_sieve_shape<SieveWide>(low, high, span, out, cursor, deep, as_stream(stream));
+    return launch_sieve_shape<SieveNarrow>(low, high, span, out, cursor, deep, as_stream(stream));
 }
 
 extern "C" {

@@ -11,29 +11,32 @@
 
 namespace ww {
 
-// k_sieve_prp's segment: 16384 bitmap words (64 KB, 2^20 numbers) for 512
-// threads, two CTAs and 32 warps per SM.  Measured against 8192 words for
-// 256 threads (four CTAs): the per-segment start-up work of the deep primes
-// halves, 1.6 % less time on 4e9 numbers below 2^64.
-#ifndef WW_SIEVE_WORDS
-#define WW_SIEVE_WORDS 16384
-#endif
-#ifndef WW_SIEVE_THREADS
-#define WW_SIEVE_THREADS 512
-#endif
-constexpr int kSegWords = WW_SIEVE_WORDS;
-constexpr int kSegOdd = kSegWords * 32;       // odd numbers per segment
-constexpr int kSieveThreads = WW_SIEVE_THREADS;
-constexpr int kSieveWarps = kSieveThreads / 32;
-constexpr int kWordsPerThread = kSegWords / kSieveThreads;
-static_assert(kSegWords % kSieveThreads == 0 && kSegWords % 32 == 0, "sieve geometry");
+
 // A warp queue holds the < 32 candidates carried over plus one chunk of 32
 // words (1024 odd numbers).  Among any 1024 consecutive odd numbers at most
 // 378 have no factor 3..17 (the maximum over the full period 3*5*...*17), so
 // 31 + 378 entries always suffice.
 constexpr int kQueueCap = 416;
-// dynamic shared memory of k_sieve_prp: the bitmap, then the warp queues
-constexpr size_t kSieveSmem = (size_t)kSegWords * 4 + (size_t)kSieveWarps * kQueueCap * 4;
+
+// A segment shape of k_sieve_prp: W bitmap words (32 W odd numbers) for T
+// threads; its dynamic shared memory is the bitmap, then one queue per warp.
+template <int W, int T>
+struct SieveGeom {
+    static constexpr int kWords = W;
+    static constexpr int kThreads = T;
+    static constexpr int kOdd = W * 32;
+    static constexpr int kWarps = T / 32;
+    static constexpr int kWordsPerThread = W / T;
+    static constexpr size_t kSmem = (size_t)W * 4 + (size_t)(T / 32) * kQueueCap * 4;
+    static_assert(W % T == 0 && W % 32 == 0 && T % 32 == 0, "sieve geometry");
+};
+// 2^20 numbers per segment for 512 threads, two CTAs and 32 warps per SM:
+// against 2^19 for 256 threads (four CTAs) the deep primes' per-segment
+// start-up work halves, 1.6 % less time on 4e9 numbers below 2^64.
+typedef SieveGeom<16384, 512> SieveWide;
+// 2^19 numbers for 256 threads: twice the segments, for ranges that would
+// not give every resident CTA of the wide shape a segment.
+typedef SieveGeom<8192, 256> SieveNarrow;
 #ifndef WW_TEST_THREADS
 #define WW_TEST_THREADS 256
 #endif

@@ -1,7 +1,7 @@
 // ww_kernels.cuh -- kernels of the WWocl search path on sm_100a.
 //
 //   k_sieve_prp   getsegprimes (getsegprimes.cl:228-301): a CTA sieves one
-//                 segment of 2*kSegOdd integers at a time (taken from a cursor,
+//                 segment of 2*G::kOdd integers at a time (taken from a cursor,
 //                 or by grid stride).  The odd numbers of the segment form a
 //                 shared-memory bitmap; each thread ORs the composite patterns
 //                 of 3..113 into its words (the reference's 27 constant tables,
@@ -22,18 +22,18 @@
 
 namespace ww {
 
-// Sieve + SPRP over [lo, hi).  b0 = lo & ~1; segment s holds the odd numbers
-// b0 + 2(s*kSegOdd + j) + 1, j < kSegOdd.
+// Sieve + SPRP over [lo, hi) in segments of shape G (SieveGeom).  b0 = lo & ~1;
+// segment s holds the odd numbers b0 + 2(s*G::kOdd + j) + 1, j < G::kOdd.
 // With a segment cursor (zeroed before the launch) the CTAs take segments
 // one at a time from it; without one (a launch captured into a graph, or
 // one that found every cursor of the library's pool busy) they stride over
 // the segments.
-__global__ void __launch_bounds__(kSieveThreads, 2048 / kSieveThreads / 2) k_sieve_prp(u64 lo, u64 hi, u64 nseg,
-                                                                                       PrpOut out, u64 *cursor,
-                                                                                       const DeepRow *deep) {
-    extern __shared__ u32 sieve_smem[];  // kSieveSmem bytes
+template <class G>
+__global__ void __launch_bounds__(G::kThreads, 1024 / G::kThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out,
+                                                                              u64 *cursor, const DeepRow *deep) {
+    extern __shared__ u32 sieve_smem[];  // G::kSmem bytes
     u32 *bitmap = sieve_smem;
-    u32(*queue)[kQueueCap] = reinterpret_cast<u32(*)[kQueueCap]>(sieve_smem + kSegWords);
+    u32(*queue)[kQueueCap] = reinterpret_cast<u32(*)[kQueueCap]>(sieve_smem + G::kWords);
     __shared__ u32 s_chunk;
     __shared__ u64 s_seg;
     const u64 b0 = lo & ~1ull;
@@ -48,19 +48,19 @@ __global__ void __launch_bounds__(kSieveThreads, 2048 / kSieveThreads / 2) k_sie
         seg = s_seg;
     }
     while (seg < nseg) {
-        const u64 seg_off = seg * (u64)(2 * kSegOdd);
+        const u64 seg_off = seg * (u64)(2 * G::kOdd);
         const u64 rem_span = span - seg_off;  // > 0
-        const u64 nvalid = (rem_span / 2 < (u64)kSegOdd) ? rem_span / 2 : (u64)kSegOdd;
+        const u64 nvalid = (rem_span / 2 < (u64)G::kOdd) ? rem_span / 2 : (u64)G::kOdd;
 
         // ---- pre-sieve 3..113 on this thread's contiguous words
         {
-            const int w0 = threadIdx.x * kWordsPerThread;
+            const int w0 = threadIdx.x * G::kWordsPerThread;
             const u64 n0 = b0 + seg_off + 64ull * (u64)w0 + 1;  // may wrap past 2^64 beyond hi
 #define WW_J0(R) u32 j##R = first_hit<R>(n0);
             WW_FOR_SMALL_PRIMES(WW_J0)
 #undef WW_J0
 #pragma unroll 4
-            for (int w = w0; w < w0 + kWordsPerThread; ++w) {
+            for (int w = w0; w < w0 + G::kWordsPerThread; ++w) {
                 u32 m = 0;
 #define WW_MASK(R) m |= prime_mask<R>(j##R); step_hit<R>(j##R);
                 WW_FOR_SMALL_PRIMES(WW_MASK)
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kSieveThreads, 2048 / kSieveThreads / 2) k_sie
 
         // ---- deep sieve 113 < r < 2^WW_DEEP_BITS, sparing possible pseudoprimes
         const u64 nbase = b0 + seg_off + 1;
-        deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, kSieveThreads, deep);
+        deep_mark(nbase, (u32)nvalid, bitmap, threadIdx.x, G::kThreads, deep);
         __syncthreads();
 
         // ---- warps take 32-word chunks dynamically (so they reach the next
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(kSieveThreads, 2048 / kSieveThreads / 2) k_sie
             u32 chunk = 0;
             if (lane == 0) chunk = atomicAdd(&s_chunk, 1u);
             chunk = __shfl_sync(0xffffffffu, chunk, 0);
-            const bool more = chunk < (u32)(kSegWords / 32);
+            const bool more = chunk < (u32)(G::kWords / 32);
             if (more) {
                 const int w = chunk * 32 + lane;
                 u32 cand = ~bitmap[w];
