@@ -30,10 +30,18 @@ struct SieveGeom {
     static constexpr size_t kSmem = (size_t)W * 4 + (size_t)(T / 32) * kQueueCap * 4;
     static_assert(W % T == 0 && W % 32 == 0 && T % 32 == 0, "sieve geometry");
 };
-// 2^20 numbers per segment for 512 threads, two CTAs and 32 warps per SM:
-// against 2^19 for 256 threads (four CTAs) the deep primes' per-segment
-// start-up work halves, 1.6 % less time on 4e9 numbers below 2^64.
-typedef SieveGeom<16384, 512> SieveWide;
+// 2^20 numbers per segment for 512 threads, two CTAs and 32 warps per SM.
+// Each doubling of the segment halves the deep primes' per-segment start-up
+// work: on 4e9 numbers below 2^64 in one launch, 2^19 numbers for 256
+// threads took 29.0 ms, 2^20 for 512 threads 28.6 ms, 2^21 for 1024
+// threads 28.1 ms.  But a 2^30-number launch (the checkpoint cadence) has
+// only 512 segments of 2^21 for 148 one-CTA SMs, and the plain range
+// pipeline fell from 775 M to 754 M primes/s with them.
+#ifndef WW_SIEVE_WIDE_WORDS
+#define WW_SIEVE_WIDE_WORDS 16384
+#define WW_SIEVE_WIDE_THREADS 512
+#endif
+typedef SieveGeom<WW_SIEVE_WIDE_WORDS, WW_SIEVE_WIDE_THREADS> SieveWide;
 // 2^19 numbers for 256 threads: twice the segments, for ranges that would
 // not give every resident CTA of the wide shape a segment.
 typedef SieveGeom<8192, 256> SieveNarrow;
