@@ -11,7 +11,6 @@
 
 namespace ww {
 
-
 // A warp queue holds the < 32 candidates carried over plus one chunk of 32
 // words (1024 odd numbers).  Among any 1024 consecutive odd numbers at most
 // 378 have no factor 3..17 (the maximum over the full period 3*5*...*17), so
@@ -45,6 +44,7 @@ typedef SieveGeom<WW_SIEVE_WIDE_WORDS, WW_SIEVE_WIDE_THREADS> SieveWide;
 // 2^19 numbers for 256 threads: twice the segments, for ranges that would
 // not give every resident CTA of the wide shape a segment.
 typedef SieveGeom<8192, 256> SieveNarrow;
+
 #ifndef WW_TEST_THREADS
 #define WW_TEST_THREADS 256
 #endif
