@@ -125,6 +125,10 @@ WW_HD u64 div_r64(u64 n, u64 &q_out) {
 // 2^64 mod n for odd n > 1.
 WW_HD u64 r_mod(u64 n) {
     if (n >> 63) return 0 - n;  // 2^64 - n < n
+    if (n >> 62) {              // 2^64 - 2n <= 2^63 < 2n
+        const u64 r = 0 - 2 * n;
+        return r >= n ? r - n : r;
+    }
     if (n >> 32) {
         u64 q;
         return div_r64(n, q);
@@ -358,7 +362,16 @@ WW_HD D2 m2_one(u64 p) {
         r.d1 = 1;
         return r;
     }
-    // 2^32 <= p < 2^63: 2^64 = q p + rem with q < p
+    if (p >> 62) {  // 2^64 = 2p + (2^64 - 2p), and 2^64 - 2p <= 2^63 < 2p
+        r.d0 = 0 - 2 * p;
+        r.d1 = 2;
+        if (r.d0 >= p) {
+            r.d0 -= p;
+            r.d1 = 3;
+        }
+        return r;
+    }
+    // 2^32 <= p < 2^62: 2^64 = q p + rem with q < p
     u64 q;
     r.d0 = div_r64(p, q);
     r.d1 = q;
