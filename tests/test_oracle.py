@@ -136,3 +136,25 @@ def test_random_prime_stream(oracle):
             assert c == int(ps[k])
             k += 1
         i += 1
+
+
+def test_oracle_matches_reference_code_on_random_ranges(oracle):
+    """The C restatement against the reference's own CPU code (oracle/_ref,
+    wwcpu.cpp + prime.h compiled in place) on seeded random ranges:
+    magnitudes log-uniform over [127, 2^64), widths from one number to 2e5."""
+    import math
+    import random
+
+    from oracle.oracle import RefCPU
+
+    if not RefCPU.available():
+        pytest.skip("oracle/_ref not built")
+    ref = RefCPU()
+    rng = random.Random(2027)
+    for _ in range(400):
+        lo = int(math.exp(rng.uniform(math.log(127), math.log(2**64 - 2))))
+        hi = min(lo + int(math.exp(rng.uniform(0, math.log(2e5)))), 2**64 - 1)
+        mine, _, _ = oracle.scan_range(lo, hi)
+        theirs = ref.scan_range(lo, hi)
+        assert (mine["prp_count"], mine["checksum"], mine["cpu_results"]) == \
+               (theirs["prp_count"], theirs["checksum"], theirs["cpu_results"]), (lo, hi)
