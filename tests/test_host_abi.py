@@ -10,7 +10,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import PKG, ROOT, sample_names
+from conftest import PKG, sample_names
 
 
 def test_library_exports_header_symbols(ww):

@@ -12,7 +12,6 @@ from __future__ import annotations
 
 import ctypes as C
 
-import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
