@@ -103,3 +103,21 @@ def test_testprimes_checks_every_segment(ref_ranges, tmp_path):
     assert out.stdout.count("GPU primes match CPU") >= 3
     lines = (tmp_path / "results-WW.txt").read_text().splitlines()
     assert lines[-1] == r["checksum"]
+
+
+@pytest.mark.parametrize("name", ["config1_5e7", "wss_special_window", "long"])
+def test_dropin_example_matches_reference(ref_ranges, tmp_path, name):
+    """bin/dropin_example, the reference program's device loop rewired onto
+    the kernel-shaped launchers in C++ (host/dropin_example.cpp), prints the
+    reference's PRP count, result count and checksum."""
+    import json
+
+    if name == "long":
+        r = json.loads((PKG.parent / "tests" / "golden" / "ref_long.json").read_text())["config3"]
+    else:
+        r = ref_ranges[name]
+    p = subprocess.run([str(PKG / "bin" / "dropin_example"), str(r["lo"]), str(r["hi"])], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    assert p.stdout.split() == ["prps", str(r["prp_count"]), "results", str(r["cpu_results"]),
+                                "checksum", r["checksum"]]
