@@ -279,3 +279,58 @@ def test_status_strings(ww):
     seen = {code: L.ww_status_string(code).decode() for code in range(-9, 1)}
     assert seen[0] == "ok" and len(set(seen.values())) == len(seen)
     assert L.ww_status_string(-100).decode() == "unknown status"
+
+
+def test_cli_host_range_split(tmp_path):
+    """The CLI's host side splits a range over host threads
+    (host/wwhost.hpp): the pieces tile [lo, hi) exactly, and the CPU prime
+    list built from them equals one built in a single pass, near 2^64 and
+    at the ranges' smallest start."""
+    src = tmp_path / "split.cpp"
+    src.write_text(r'''
+#include <stdio.h>
+#include <mutex>
+#include "wwhost.hpp"
+using namespace wwhost;
+static std::vector<uint64_t> single(uint64_t lo, uint64_t hi) {
+    std::vector<uint64_t> out;
+    for (uint64_t n = lo | 1; n < hi && n >= lo; n += 2) {
+        bool small = false;
+        for (uint32_t r = 3; r <= 113 && !small; r += 2) small = (n % r == 0) && n != r;
+        if (!small && n > 113 && ww_is_prime(n)) out.push_back(n);
+        if (n > UINT64_MAX - 2) break;
+    }
+    return out;
+}
+int main() {
+    const uint64_t cases[][2] = {{127, 300000}, {18446744073708551615ull - 2000000, 18446744073709551615ull},
+                                 {1000000007, 1000000008}, {5000, 5000 + 65536 * 3 + 1}};
+    for (auto &c : cases) {
+        std::mutex m;
+        std::vector<std::pair<uint64_t, uint64_t>> pieces;
+        parallel_pieces(c[0], c[1], [&](uint64_t a, uint64_t b, unsigned) {
+            std::lock_guard<std::mutex> g(m);
+            pieces.push_back({a, b});
+        });
+        std::sort(pieces.begin(), pieces.end());
+        uint64_t at = c[0];
+        for (auto &p : pieces) {
+            if (p.first != at || p.second <= p.first) return printf("bad piece\n"), 1;
+            at = p.second;
+        }
+        if (at != c[1]) return printf("gap at the end\n"), 1;
+        if (cpu_primes(c[0], c[1]) != single(c[0], c[1])) return printf("prime list differs\n"), 1;
+    }
+    printf("ok\n");
+    return 0;
+}
+''')
+    exe = tmp_path / "split"
+    inc = PKG / "host"
+    cuda_inc = "/usr/local/cuda/include"
+    b = subprocess.run(["g++", "-O2", "-std=c++17", "-pthread", f"-I{inc}", f"-I{PKG.parent / 'include'}",
+                        f"-I{cuda_inc}", str(src), "-o", str(exe), f"-L{PKG / 'lib'}", "-lwwcuda",
+                        f"-Wl,-rpath,{PKG / 'lib'}"], capture_output=True, text=True)
+    assert b.returncode == 0, b.stderr[-2000:]
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr

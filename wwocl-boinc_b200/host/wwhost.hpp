@@ -1,6 +1,6 @@
 // wwhost.hpp -- host services of the wwocl program: A/B checkpoint files,
-// the results file, the CPU prime list used to check the GPU PRP list, and
-// a monotonic clock.  Behaviour follows the reference's main.cpp; every
+// the results file, the CPU prime list used to check the GPU PRP list, the
+// split of a range over host threads, and a monotonic clock.  Behaviour follows the reference's main.cpp; every
 // function cites the lines it mirrors.
 #pragma once
 
@@ -13,9 +13,9 @@
 #include <unistd.h>
 
 #include <algorithm>
-#include <thread>
 #include <chrono>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "boinc_shim.hpp"
