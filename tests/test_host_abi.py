@@ -334,3 +334,49 @@ int main() {
     assert b.returncode == 0, b.stderr[-2000:]
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
+
+
+def _primes_near(oracle, x: int, count: int, up: bool = True) -> list[int]:
+    out, n = [], x | 1
+    while len(out) < count and 127 <= n < 2**64:
+        if oracle.is_prime(n):
+            out.append(n)
+        n += 2 if up else -2
+    return out
+
+
+def test_host_twin_ladder_start_edges(ww, oracle):
+    """The ladders start from the top bits of their exponents (a Lucas number
+    or a power of two times the Montgomery one, reduced with a double-precision
+    quotient estimate).  Primes where that start is least ordinary: every
+    prime below 20000, the Mersenne primes whose p + 1 is a power of two
+    (the Lucas index then has two bits more than (p-1)/2), and primes on both
+    sides of each power of two from 2^7 to 2^64."""
+    ps = [n for n in range(127, 20000, 2) if oracle.is_prime(n)]
+    ps += [2**7 - 1, 2**13 - 1, 2**17 - 1, 2**19 - 1, 2**31 - 1, 2**61 - 1]
+    for b in range(8, 65):
+        ps += _primes_near(oracle, 2**b - 1, 6, up=False)
+        if b < 64:
+            ps += _primes_near(oracle, 2**b + 1, 6, up=True)
+    ps = np.array(sorted(set(ps)), dtype=np.uint64)
+    d = ww.selftest_digits(ps)
+    w, s = oracle.list_digits(ps)
+    assert np.array_equal(d[:, 0:2], w)
+    assert np.array_equal(d[:, 2:4], s)
+
+
+@pytest.mark.parametrize("lo,hi", [(127, 40000), (2**13 - 200, 2**13 + 200), (2**19 - 300, 2**19 + 300),
+                                   (2**31 - 400, 2**31 + 400), (2**32 - 20000, 2**32 + 20000),
+                                   (2**61 - 30000, 2**61 + 30000), (2**62 - 20000, 2**62 + 20000),
+                                   (2**63 - 20000, 2**63 + 20000)])
+def test_host_twin_range_at_boundaries(ww, oracle, lo, hi):
+    """The SPRP test starts after the top five bits of n-1 when its 2-adic
+    valuation lies below them (the pseudoprime 2^32 + 1, whose n-1 is a power
+    of two, takes the other start), the separate Wieferich and Wall-Sun-Sun
+    ladders from their top bits: PRP count, checksum and hits of ranges across
+    powers of two (and Mersenne primes) equal the oracle's."""
+    got = ww.selftest_range(lo, hi)
+    want, _, _ = oracle.scan_range(lo, hi)
+    assert got["prp_count"] == want["prp_count"]
+    assert got["checksum"] == want["checksum"]
+    assert got["result_count"] == want["gpu_results"]

@@ -136,12 +136,51 @@ WW_HD u64 r_mod(u64 n) {
     return (0 - n) % n;
 }
 
+// T mod n and floor(T / n) for T = h 2^64 + l < 2^46 n, n odd and > 1, with
+// rn = 1.0 / (double)n.  The quotient (below 2^46) is estimated in double
+// precision: T and rn each carry a relative rounding error of at most 2^-52
+// and the product one more rounding, so the estimate is within 2^-4 of T / n
+// and its truncation is the quotient or one off it; T - qe n then lies in
+// [-n, 2n) and one exact correction finishes.  Host and device run the same
+// steps.  This is how the ladders start from their top bits (a small power
+// or Lucas number times the Montgomery one) without a division loop.
+WW_HD u64 mod_est(u64 h, u64 l, u64 n, double rn, u64 &quot) {
+    const double t = (double)h * 18446744073709551616.0 + (double)l;
+    u64 qe = (u64)(t * rn);
+    const u64 ql = qe * n;
+    u64 lo = l - ql;
+    const u64 hi = h - mul_hi(qe, n) - (u64)(l < ql);  // (hi:lo) = T - qe n
+    if ((long long)hi < 0) {
+        lo += n;
+        --qe;
+    } else if (hi != 0 || lo >= n) {
+        lo -= n;
+        ++qe;
+    }
+    quot = qe;
+    return lo;
+}
+
+// Where the base-2 powering of the SPRP test starts: after the top five bits
+// v of n-1 (2^v R mod n from one exact reduction, mod_est) when the 2-adic
+// valuation t of n-1 lies below them, which saves the first four squarings;
+// otherwise after the leading bit.  Returns s, the loop then takes the bits
+// s-1 .. 1 of n-1; a receives the start value.
+WW_HD int sprp2_start(u64 n, u64 one, int top, int t, u64 &a) {
+    const int s = (top - 4 > t) ? top - 4 : top;
+    const u32 v = (u32)((n - 1) >> s);  // in [16, 32), or 1
+    u64 qd;
+    a = mod_est(one >> (64 - v), one << v, n, 1.0 / (double)n, qd);
+    return s;
+}
+
 // Base-2 strong probable-prime test (prime.h:65-114, getsegprimes.cl:118-164)
 // written as one uniform loop over the bits of n-1 so that a warp's lanes
 // stay converged whatever the 2-adic valuation t of n-1 is: the trailing t
 // zero bits square without doubling; the loop keeps a^d (the value at bit t)
 // and whether a^(d 2^s) = -1 below it, and the checks run once at the end.
-// Returns the result and n^-1 mod 2^64.
+// The powering starts from the top bits of n-1 (sprp2_start).  Returns the
+// result and n^-1 mod 2^64.
 WW_HD bool sprp2(u64 n, u64 &q_out) {
     const u64 q = inv64(n);
     q_out = q;
@@ -155,10 +194,11 @@ WW_HD bool sprp2(u64 n, u64 &q_out) {
     const int t = __builtin_ctzll(nm1);
     const int top = 63 - __builtin_clzll(nm1);
 #endif
-    u64 a = add_mod(one, one, n);  // 2 for the leading bit
+    u64 a;
+    const int s = sprp2_start(n, one, top, t, a);
     u64 at_t = 0;                  // 2^d, the value at bit t
     bool m1 = false;               // 2^(d 2^s) = -1 for some 0 < s < t
-    for (int i = top - 1; i >= 1; --i) {
+    for (int i = s - 1; i >= 1; --i) {
         a = mont_mul(a, a, n, q);
         const u64 d = add_mod(a, a, n);
         a = ((nm1 >> i) & 1) ? d : a;
@@ -167,7 +207,8 @@ WW_HD bool sprp2(u64 n, u64 &q_out) {
     }
     bool ok = (at_t == one) | (at_t == mone) | m1;
     if (t == 0) ok = false;  // even n is never a candidate
-    // t == top (n-1 a power of two) never happens for the odd n >= 127 tested
+    // t == top (n-1 a power of two, as for the pseudoprime 2^32+1): the value
+    // at bit t is 2, never +-1, and m1 covers every s < t
     return ok;
 }
 
@@ -193,9 +234,10 @@ __device__ __forceinline__ bool sprp2_warp(u64 n, bool act, u64 &q_out) {
     const int t = __ffsll((long long)nm1) - 1;  // >= 1: n is odd
     const int top = 63 - __clzll((long long)nm1);
     const int tw = (int)__reduce_max_sync(0xffffffffu, (unsigned)t);
-    u64 a = add_mod(one, one, n);
-    u64 ebits = nm1 << (64 - top);  // bit top-1 of n-1 at bit 63
-    int i = top - 1;
+    u64 a;
+    const int s = sprp2_start(n, one, top, t, a);
+    u64 ebits = nm1 << (64 - s);  // bit s-1 of n-1 at bit 63
+    int i = s - 1;
     for (; i > tw; --i) {
         a = mont_mul(a, a, n, q);
         const u64 d = add_mod(a, a, n);
@@ -375,6 +417,21 @@ WW_HD D2 m2_one(u64 p) {
     u64 q;
     r.d0 = div_r64(p, q);
     r.d1 = q;
+    return r;
+}
+
+// L R mod p^2 as canonical digits for L < 2^45, from the Montgomery one
+// (R mod p^2 = o0 + p o1): L o0 = d0 + p q0 with d0 < p, then d1 = (q0 + L o1)
+// mod p.  Both reductions see a number below 2^46 p (mod_est); rp = 1/(double)p.
+WW_HD D2 m2_small(u64 L, D2 one, u64 p, double rp) {
+    u64 l, h, q0, q1;
+    D2 r;
+    mul_wide(L, one.d0, l, h);
+    r.d0 = mod_est(h, l, p, rp, q0);
+    mul_wide(L, one.d1, l, h);
+    l += q0;
+    h += (u64)(l < q0);
+    r.d1 = mod_est(h, l, p, rp, q1);
     return r;
 }
 

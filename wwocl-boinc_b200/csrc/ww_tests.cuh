@@ -75,15 +75,71 @@ WW_HD D2 sel(bool c, D2 a, D2 b) {
     return r;
 }
 
+// Lucas numbers V_k (P = 1, Q = -1: V_0 = 2, V_1 = 1) for 32 <= k <= 64, all
+// below 2^45: the Lucas ladder's state after the top six bits of its index.
+#define WW_LUCAS_32_64                                                                                \
+    4870847ull, 7881196ull, 12752043ull, 20633239ull, 33385282ull, 54018521ull, 87403803ull,        \
+        141422324ull, 228826127ull, 370248451ull, 599074578ull, 969323029ull, 1568397607ull,        \
+        2537720636ull, 4106118243ull, 6643838879ull, 10749957122ull, 17393796001ull, 28143753123ull, \
+        45537549124ull, 73681302247ull, 119218851371ull, 192900153618ull, 312119004989ull,          \
+        505019158607ull, 817138163596ull, 1322157322203ull, 2139295485799ull, 3461452808002ull,     \
+        5600748293801ull, 9062201101803ull, 14662949395604ull, 23725150497407ull
+#if defined(__CUDACC__)
+static __device__ const u64 g_lucas_32_64[33] = {WW_LUCAS_32_64};
+#endif
+static const u64 h_lucas_32_64[33] = {WW_LUCAS_32_64};
+
+WW_HD u64 lucas_small(u32 k) {  // 32 <= k <= 64
+#if defined(__CUDA_ARCH__)
+    return __ldg(&g_lucas_32_64[k - 32]);
+#else
+    return h_lucas_32_64[k - 32];
+#endif
+}
+
+// Where the ladders start.  Each takes the bits of its exponent below its
+// start bit in the loop and begins from the value of the bits above it:
+//   Lucas: i0 = top_bit(n) - 6 for n = p - (p|5); k0 = n >> (i0 + 1) is the
+//          top six bits of n (32 <= k0 < 64), so the pair (V_k0, V_k0+1)
+//          comes from lucas_small;
+//   Wieferich: iw = top_bit(e) - 5 for e = (p-1)/2; e0 = e >> (iw + 1) is the
+//          top five bits of e (16 <= e0 < 32), so the start is 2^e0.
+// e has one bit fewer than n, so iw = i0 (two fewer when p + 1 is a power of
+// two, and then the first loop step is the Lucas ladder's alone).  m2_small
+// turns each start into Montgomery form with two exact reductions: six
+// reductions of about 25 instructions replace the first five ladder steps
+// (ten squarings) and four Wieferich squarings.
+struct LadderStart {
+    int i0, iw;
+    bool odd;  // parity of the Lucas index k0
+    D2 a, b, w;
+};
+
+WW_HD LadderStart ladder_start(u64 p, u64 n, D2 one) {
+    LadderStart st;
+    const u64 e = p >> 1;
+    st.i0 = top_bit(n) - 6;
+    st.iw = top_bit(e) - 5;
+    const u32 k0 = (u32)(n >> (st.i0 + 1));
+    const u32 e0 = (u32)(e >> (st.iw + 1));
+    const double rp = 1.0 / (double)p;
+    st.odd = k0 & 1u;
+    st.a = m2_small(lucas_small(k0), one, p, rp);
+    st.b = m2_small(lucas_small(k0 + 1), one, p, rp);
+    st.w = m2_small(1ull << e0, one, p, rp);
+    return st;
+}
+
 // 2^((p-1)/2) mod p^2 as canonical digits: left-to-right powering of 2, a
 // squaring per exponent bit and a doubling where the bit is set
-// (wieferich.cl:219-245).
+// (wieferich.cl:219-245), from 2^e0 for the top five bits e0 of the exponent.
 template <class A>
 WW_HD D2 wieferich_digits_t(u64 p, u64 q, D2 one) {
     const A ar(p, q);
     const u64 e = p >> 1;
-    D2 a = m2_dbl(one, p);
-    for (int i = top_bit(e) - 1; i >= 0; --i) {
+    const int i0 = top_bit(e) - 5;
+    D2 a = m2_small(1ull << (u32)(e >> (i0 + 1)), one, p, 1.0 / (double)p);
+    for (int i = i0; i >= 0; --i) {
         a = ar.sqr(a);
         a = sel((e >> i) & 1, m2_dbl(a, p), a);
     }
@@ -96,7 +152,8 @@ WW_HD D2 wieferich_digits_t(u64 p, u64 q, D2 one) {
 // on (V_k, V_{k+1}) with two squarings per bit:
 //   V_2k = V_k^2 - 2(-1)^k,  V_2k+2 = V_k+1^2 + 2(-1)^k,  V_2k+1 = V_2k+2 - V_2k,
 // and F_n = (2 V_{n+1} - V_n) / 5 gives the same residue exactly (5 is a
-// unit mod p^2 since p has no factor below 127).
+// unit mod p^2 since p has no factor below 127).  The ladder starts from
+// the top six bits of n (ladder_start).
 template <class A>
 WW_HD D2 wss_digits_t(u64 p, u64 q, D2 one) {
     const A ar(p, q);
@@ -105,10 +162,13 @@ WW_HD D2 wss_digits_t(u64 p, u64 q, D2 one) {
     const D2 zero = {0, 0};
     const D2 two = m2_dbl(one, p);
     const D2 mtwo = m2_sub(zero, two, p);
-    D2 a = one;                  // V_1
-    D2 b = m2_add(two, one, p);  // V_2
-    bool odd = true;             // parity of the ladder index k
-    for (int i = top_bit(n) - 1; i >= 0; --i) {
+    const int i0 = top_bit(n) - 6;
+    const u32 k0 = (u32)(n >> (i0 + 1));
+    const double rp = 1.0 / (double)p;
+    D2 a = m2_small(lucas_small(k0), one, p, rp);      // V_k0
+    D2 b = m2_small(lucas_small(k0 + 1), one, p, rp);  // V_k0+1
+    bool odd = k0 & 1u;  // parity of the ladder index k
+    for (int i = i0; i >= 0; --i) {
         const bool bit = (n >> i) & 1;
         const D2 c = sel(odd, two, mtwo);  // -2(-1)^k
         const D2 v2k = m2_add(ar.sqr(a), c, p);
@@ -128,26 +188,26 @@ WW_HD D2 wss_digits_t(u64 p, u64 q, D2 one) {
 //   V_2k = V_k^2 - 2(-1)^k,  V_2k+2 = V_k+1^2 + 2(-1)^k,
 //   V_2k+1 = V_2k+2 - V_2k   (the recurrence V_m+1 = V_m + V_m-1),
 // so the three products of an iteration are squarings, independent of each
-// other, and no operand has to be selected before multiplying.  The Lucas
-// exponent is one or two bits longer; its first steps run alone.
+// other, and no operand has to be selected before multiplying.  Both start
+// from their top bits (ladder_start), the Wieferich powering at most one
+// bit after the ladder.
 template <class A>
 WW_HD void both_digits_t(u64 p, u64 q, D2 one, D2 &s_out, D2 &c_out) {
     const A ar(p, q);
     const u32 pm5 = (u32)(p % 5);
     const u64 n = (pm5 == 2 || pm5 == 3) ? p + 1 : p - 1;
     const u64 e = p >> 1;
-    const int top_e = top_bit(e);
     const D2 zero = {0, 0};
     const D2 two = m2_dbl(one, p);
     const D2 mtwo = m2_sub(zero, two, p);
-    D2 a = one, b = m2_add(two, one, p);  // V_1, V_2
-    D2 w = two;
-    bool odd = true;  // parity of the ladder index k
-    for (int i = top_bit(n) - 1; i >= 0; --i) {
+    const LadderStart st = ladder_start(p, n, one);
+    D2 a = st.a, b = st.b, w = st.w;
+    bool odd = st.odd;
+    for (int i = st.i0; i >= 0; --i) {
         const bool bit = (n >> i) & 1;
         const D2 a2 = ar.sqr(a);
         const D2 b2 = ar.sqr(b);
-        if (i < top_e) {
+        if (i <= st.iw) {
             w = ar.sqr(w);
             w = sel((e >> i) & 1, m2_dbl(w, p), w);
         }
