@@ -13,9 +13,12 @@ scaling, no data-path collective.  Rank 0 prints one JSON line, which at
 N = 1 also carries: `roofline` (the test kernel against the measured
 integer-multiply chain peak), `cpu_baseline` (the reference's own CPU code on
 the host cores), `range_pipeline` (the plain path over the 2^34-wide range
-below 2^64, checksum against the reference), `batched_vs_plain` (the uneven
-mix: batched engine vs one launch sequence per range, vs one program run per
-range) and `serving` (Poisson request stream, p50/p99 latency).
+below 2^64, checksum against the reference), `batched_vs_plain` (all 4096
+units of the uneven mix: batched engine vs one launch sequence per range in
+the same process; one program run per range as a deployment note) and
+`serving` (the 120-s Poisson request stream, p50/p99 latency), and last a
+short `summary` of every leg.  The default run takes about eight minutes;
+--batch-units / --serve-seconds / --range-width shorten or skip the legs.
 """
 from __future__ import annotations
 
@@ -59,10 +62,10 @@ def parse_args():
                     help="width of the plain-path range leg starting at 2^64-2^35 (0: skip)")
     ap.add_argument("--batch-config", default="",
                     help="force the batched configuration SEG_WORDS/THREADS/PPT instead of the autotuner's choice")
-    ap.add_argument("--batch-units", type=int, default=128,
-                    help="units of the uneven mix for the batched-vs-plain line (0: skip)")
-    ap.add_argument("--serve-seconds", type=float, default=10.0,
-                    help="length of the Poisson request stream (0: skip)")
+    ap.add_argument("--batch-units", type=int, default=4096,
+                    help="units of the seed-11 uneven mix for the batched-vs-plain leg (4096: the whole mix; 0: skip)")
+    ap.add_argument("--serve-seconds", type=float, default=120.0,
+                    help="length of the Poisson request stream (120: the whole stream; 0: skip)")
     return ap.parse_args()
 
 
@@ -89,12 +92,14 @@ def algorithmic_imad_per_prime(primes: np.ndarray) -> tuple[float, float]:
       reference_count: the reference kernels' algorithm -- Wieferich k-3
         squarings (wieferich.cl:196-328), the Lucas ladder k-1 steps of two
         squarings and one product (wallsunsun.cl:221-354): 40(k-3) + 128(k-1).
-      executed_count: what k_test_prps runs -- Wieferich k-2 squarings, the
-        Lucas ladder k-1 steps of two squarings, two conversions out of
-        Montgomery form (24 each): 40(k-2) + 80(k-1) + 48."""
+      executed_count: what k_test_prps runs -- both ladders start from the
+        top bits of their exponents (three small numbers turned into
+        Montgomery form, 40 each), then Wieferich k-6 squarings and the Lucas
+        ladder k-6 steps of two squarings, two conversions out of Montgomery
+        form (24 each): 120(k-6) + 120 + 48."""
     bits = np.floor(np.log2(primes.astype(np.float64))) + 1  # exact away from powers of two
     ref = 40.0 * (bits - 3) + 128.0 * (bits - 1)
-    run = 40.0 * (bits - 2) + 80.0 * (bits - 1) + 48.0
+    run = 120.0 * (bits - 6) + 168.0
     return float(ref.mean()), float(run.mean())
 
 
@@ -203,7 +208,8 @@ def run_reference(args):
     return 0
 
 
-def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30, chain_peak: float | None = None) -> dict:
+def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30, chain_peak: float | None = None,
+                       depth: int = 20) -> dict:
     """The plain one-range path over [2^64-2^35, 2^64-2^35+width): per 2^30
     numbers (the checkpoint cadence) clear, sieve + SPRP, both tests, sync and
     read the counters back, as the reference program's loop does.  With the
@@ -255,15 +261,16 @@ def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30, chain_pe
            "checksum": "%016X" % cks, "results": res}
     if chain_peak:
         # end to end over sieve + tests, in the same 32-bit multiply units as
-        # the test kernel's roofline (k = 64 here): the SPRP of a candidate is
-        # 20(k-1); the reference's sieve hands ~5.3 candidates per PRP to it,
-        # the deep sieve here ~1.8 (0.5615 / ln 2^20 per integer over the PRP
-        # density 1 / ln 2^64)
+        # the test kernel's roofline (k = 64 here): the reference's SPRP of a
+        # candidate is 20(k-1) and its sieve hands ~5.3 candidates per PRP to
+        # it; here the SPRP starts after the top five bits of n-1 (20(k-5)
+        # plus a 12-multiply start) and the deep sieve to 2^depth leaves
+        # 0.5615 / ln 2^depth candidates per integer, against the PRP density
+        # 1 / ln 2^64
         k = 64
-        sprp = 20.0 * (k - 1)
-        ref_ops = 40.0 * (k - 3) + 128.0 * (k - 1) + 5.3 * sprp
-        cand = (0.5615 / np.log(2.0**20)) * np.log(2.0**64)
-        run_ops = 40.0 * (k - 2) + 80.0 * (k - 1) + 48.0 + cand * sprp
+        ref_ops = 40.0 * (k - 3) + 128.0 * (k - 1) + 5.3 * 20.0 * (k - 1)
+        cand = (0.5615 / np.log(2.0**depth)) * np.log(2.0**64)
+        run_ops = 120.0 * (k - 6) + 168.0 + cand * (20.0 * (k - 5) + 12.0)
         rate = out["primes_per_s"]
         out["roofline_end_to_end"] = {
             "peak_tops": chain_peak / 1e12,
@@ -280,11 +287,15 @@ def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30, chain_pe
 
 
 def compare_batched_plain(ww, local: int, units: list, workload: str, tune_units: int = 32,
-                          force_cfg: tuple | None = None) -> dict:
+                          force_cfg: tuple | None = None, fused_units: int | None = None) -> dict:
     """Plain = one range per launch sequence (clear, sieve, test, read)
     through the context API; batched = one persistent CUDA-graph launch over
     the tile queue after the autotuner picked the configuration.  Per-unit
-    checksums and PRP counts must agree."""
+    checksums, PRP counts and hit counts must agree.  The batched launch is
+    warmed on a subset of the units (the autotuner has already run every
+    configuration), so at the mix's full size each path runs once.
+    fused_units: how many of the units also run one launch sequence per range
+    with the fused test kernel (None: all)."""
     ctx = ww.Context(local, max_prps=ww.prp_count_bound(0, 1 << 30), max_hits=15000)
     b = ww.Batch(ctx)
     if force_cfg:
@@ -292,7 +303,7 @@ def compare_batched_plain(ww, local: int, units: list, workload: str, tune_units
         cfg = b.config()
     else:
         cfg, _ = b.tune(units[:tune_units])
-    b.run(units)  # warm
+    b.run(units[:64])  # warm: graph capture of the batched launch
     ctx.marker(0)
     res = b.run(units)
     ctx.marker(1)
@@ -324,24 +335,27 @@ def compare_batched_plain(ww, local: int, units: list, workload: str, tune_units
             start = stop
         plain.append((cks, cnt, hits))
     plain_s = time.perf_counter() - t0
+    equal = all((r["checksum"], r["prp_count"], r["hits"]) == p for r, p in zip(res, plain))
     # the same ranges one per launch sequence with the fused test kernel
+    nf = len(units) if fused_units is None else min(fused_units, len(units))
     t0 = time.perf_counter()
-    alone = [ctx.run_range(a, z) for a, z in units]
+    alone = [ctx.run_range(a, z) for a, z in units[:nf]]
     fused_s = time.perf_counter() - t0
-    equal = all(r["checksum"] == a["checksum"] and r["prp_count"] == a["total_prp_count"] and
-                r["hits"] == a["result_count"] and (r["checksum"], r["prp_count"], r["hits"]) == p
-                for r, a, p in zip(res, alone, plain))
+    equal_fused = all(r["checksum"] == a["checksum"] and r["prp_count"] == a["total_prp_count"] and
+                      r["hits"] == a["result_count"] for r, a in zip(res, alone))
     ctx.close()
     numbers = sum(z - a for a, z in units)
+    fused_prps = sum(r["prp_count"] for r in res[:nf])
+    ratio = plain_s / (batch_ms * 1e-3)
     return {"workload": workload, "units": len(units),
             "numbers": numbers, "prps": prps, "batched_primes_per_s": prps / (batch_ms * 1e-3),
-            "plain_primes_per_s": prps / plain_s, "plain_fused_primes_per_s": prps / fused_s,
-            "batched_numbers_per_s": numbers / (batch_ms * 1e-3),
-            "speedup_batched_vs_plain": plain_s / (batch_ms * 1e-3),
-            "speedup_batched_vs_plain_fused": fused_s / (batch_ms * 1e-3),
+            "plain_primes_per_s": prps / plain_s, "batched_numbers_per_s": numbers / (batch_ms * 1e-3),
+            "speedup_batched_vs_plain": ratio, "target_1p5x_met": bool(ratio >= 1.5),
             "plain_definition": "per range: sieve, Wieferich, WSS kernels; checkpoint sync + read-back "
-                                "every 2^30 numbers (the reference program's loop)",
-            "per_unit_bit_identical": bool(equal),
+                                "every 2^30 numbers (the reference program's loop), in the same process",
+            "per_unit_bit_identical": bool(equal and equal_fused),
+            "plain_fused": {"units": nf, "primes_per_s": fused_prps / fused_s if nf else None,
+                            "definition": "per range: sieve, fused Wieferich+WSS kernel, read-back"},
             "tuned_config": {"seg_words": cfg[0], "seg_bytes": 4 * cfg[0], "threads": cfg[1],
                              "primes_per_thread": cfg[2]}}
 
@@ -387,22 +401,24 @@ def compare_batched_per_run(ww, local: int, units: list, workload: str) -> dict:
 def run_batched_vs_plain(ww, local: int, n_units: int, force_cfg: tuple | None = None) -> dict:
     """The seed-11 uneven mix (4096 units, widths log-uniform in [1e6, 1e10],
     starts uniform in [1e15, 2^64-1e10], multiples of 30): its first n_units
-    units, and separately its first 2*n_units units narrower than 1e8 (where
-    one launch sequence per range leaves most of the GPU idle)."""
+    units (all 4096 by default), and separately its first 256 units narrower
+    than 1e8 (where one launch sequence per range leaves most of the GPU
+    idle).  The per-process comparison (one program run per range) is a
+    deployment note on 8 units, not the batching result."""
     mix = ww.uneven_units(11, 4096)
-    out = compare_batched_plain(ww, local, mix[:n_units],
-                                f"first {n_units} units of the seed-11 uneven mix (4096 units)", force_cfg=force_cfg)
-    narrow = [u for u in mix if u[1] - u[0] < 10**8][: 2 * n_units]
+    what = "all 4096 units" if n_units >= 4096 else f"first {n_units} units"
+    out = compare_batched_plain(ww, local, mix[:n_units], f"{what} of the seed-11 uneven mix", force_cfg=force_cfg,
+                                fused_units=min(n_units, 128))
+    narrow = [u for u in mix if u[1] - u[0] < 10**8][:256]
     out["narrow_units"] = compare_batched_plain(
         ww, local, narrow, f"first {len(narrow)} units of the same mix narrower than 1e8", force_cfg=force_cfg)
-    k = max(1, n_units // 16)
-    out["per_run"] = compare_batched_per_run(ww, local, mix[:k],
-                                             f"first {k} units of the same mix, one program run per range")
+    out["per_run"] = compare_batched_per_run(ww, local, mix[:8], "first 8 units of the same mix, one program "
+                                             "run per range (deployment note, not the batching target)")
     return out
 
 
 def run_serving(ww, local: int, seconds: float, rate: float = 200.0, seed: int = 13, check_cpu: int = 12):
-    """Config 5, shortened: Poisson arrivals at `rate` req/s for `seconds`,
+    """Config 5: Poisson arrivals at `rate` req/s for `seconds` (120 s in full),
     widths log-uniform in [1e5, 1e9], starts uniform in [1e12, 2^64-1e9].
     Latency = completion time - arrival time on the host monotonic clock."""
     rng = np.random.default_rng(seed)
@@ -459,6 +475,44 @@ def run_serving(ww, local: int, seconds: float, rate: float = 200.0, seed: int =
             "max_ms": float(lat.max()), "primes_per_s": prps / wall, "numbers_per_s": numbers / wall,
             "offered_numbers_per_s": numbers / seconds, "all_ok": bool(ok_status),
             "cpu_checksum_equal_on_smallest": cpu_equal}
+
+
+def summarize(line: dict, extra: dict) -> dict:
+    """Short figures of every leg, for the end of the JSON line."""
+    def r(x, d=3):
+        return None if x is None else float(f"{x:.{d}g}")
+
+    rl = line["roofline"]
+    cpu = line.get("cpu_baseline") or {}
+    out = {"config2_fixed_list": {"primes_per_s": r(line["value"], 4), "e2e_primes_per_s": r(line["e2e"]["value"], 4),
+                                  "frac_chain_peak_ref_ops": r(rl["frac"]),
+                                  "frac_chain_peak_executed": r(rl["executed"]["frac"]),
+                                  "frac_madlo_peak_ref_ops": r(rl["mad_lo_only"]["frac"]),
+                                  "frac_madlo_peak_executed": r(rl["mad_lo_only"]["frac_executed"]),
+                                  "cpu_primes_per_s": r(cpu.get("value"), 4),
+                                  "cpu_checksum_match": cpu.get("checksum_match")}}
+    if "range_pipeline" in extra:
+        g = extra["range_pipeline"]
+        out["config3_plain_range"] = {"primes_per_s": r(g["primes_per_s"], 4), "numbers_per_s": r(g["numbers_per_s"], 4),
+                                      "sieve_ms_2p30": r(g["segment_2p30"]["sieve_ms"]),
+                                      "test_ms_2p30": r(g["segment_2p30"]["test_ms"]),
+                                      "checksum": g["checksum"],
+                                      "checksum_equal_reference": g.get("reference_checksum_equal")}
+    if "batched_vs_plain" in extra:
+        g = extra["batched_vs_plain"]
+        out["config4_batched_vs_plain"] = {
+            "units": g["units"], "batched_primes_per_s": r(g["batched_primes_per_s"], 4),
+            "plain_primes_per_s": r(g["plain_primes_per_s"], 4), "ratio": r(g["speedup_batched_vs_plain"]),
+            "target_1p5x_met": g["target_1p5x_met"], "per_unit_bit_identical": g["per_unit_bit_identical"],
+            "narrow_ratio": r(g["narrow_units"]["speedup_batched_vs_plain"]),
+            "per_process_ratio_note": r(g["per_run"].get("speedup_batched_vs_per_run")),
+            "tuned": "%d/%d/%d" % tuple(g["tuned_config"][k] for k in ("seg_words", "threads", "primes_per_thread"))}
+    if "serving" in extra:
+        g = extra["serving"]
+        out["config5_serving"] = {"requests": g["requests"], "p50_ms": r(g["p50_ms"]), "p99_ms": r(g["p99_ms"]),
+                                  "max_ms": r(g["max_ms"]), "primes_per_s": r(g["primes_per_s"], 4),
+                                  "all_ok": g["all_ok"], "cpu_checksum_equal": g["cpu_checksum_equal_on_smallest"]}
+    return out
 
 
 def main():
@@ -569,7 +623,7 @@ def main():
                 "ops_source": "reference kernels' algorithm: 40(k-3) + 128(k-1) 32-bit multiplies per prime",
                 "executed": {"ops_per_prime": per_prime_run, "achieved": achieved_run / 1e12,
                              "frac": achieved_run / chain_peak,
-                             "note": "multiplies k_test_prps itself runs: 40(k-2) + 80(k-1) + 48"},
+                             "note": "multiplies k_test_prps itself runs: 120(k-6) + 168 (ladders started from their top bits)"},
                 "mad_lo_only": {"peak": madlo_peak / 1e12, "frac": achieved / madlo_peak,
                                 "frac_executed": achieved_run / madlo_peak},
                 "hbm": {"bytes_per_launch": 16 * n, "GBps": 16 * n / (launch_ms * 1e-3) / 1e9,
@@ -619,6 +673,9 @@ def main():
                             "+ ww_read_counters", "checksum_equal": bool(e2e_checksum == checksum)},
             "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu,
             "clocks": clocks.summary(), "checksum": "%016X" % checksum, "list_gen_s": gen_s}
+    # last key: every leg's results in a few hundred bytes (kept by a reader
+    # that keeps only the end of the output)
+    line["summary"] = summarize(line, extra)
     print(json.dumps(line))
     ctx.close()
     if world > 1:

@@ -51,3 +51,31 @@ def test_reference_arm_under_torchrun_prints_one_line():
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+
+
+def test_summary_is_short_and_carries_every_leg():
+    """The JSON line ends with a summary of every leg that fits in the last
+    1500 characters of the output."""
+    import importlib
+
+    sys.path.insert(0, str(ROOT))
+    bench = importlib.import_module("bench")
+    line = {"value": 1.1e9, "e2e": {"value": 1.0e9},
+            "roofline": {"frac": 0.93, "executed": {"frac": 0.64}, "mad_lo_only": {"frac": 0.62, "frac_executed": 0.43}},
+            "cpu_baseline": {"value": 5.8e6, "checksum_match": True}}
+    seg = {"sieve_ms": 7.7, "test_ms": 22.0}
+    extra = {"range_pipeline": {"primes_per_s": 8.1e8, "numbers_per_s": 3.6e10, "segment_2p30": seg,
+                                "checksum": "1715455BAC8C55C2", "reference_checksum_equal": True},
+             "batched_vs_plain": {"units": 4096, "batched_primes_per_s": 8.0e8, "plain_primes_per_s": 7.7e8,
+                                  "speedup_batched_vs_plain": 1.04, "target_1p5x_met": False,
+                                  "per_unit_bit_identical": True, "narrow_units": {"speedup_batched_vs_plain": 2.6},
+                                  "per_run": {"speedup_batched_vs_per_run": 60.0},
+                                  "tuned_config": {"seg_words": 16384, "threads": 512, "primes_per_thread": 1}},
+             "serving": {"requests": 24008, "p50_ms": 15.9, "p99_ms": 168.0, "max_ms": 394.0, "primes_per_s": 5.1e8,
+                         "all_ok": True, "cpu_checksum_equal_on_smallest": True}}
+    s = bench.summarize(line, extra)
+    text = json.dumps({"summary": s})
+    assert len(text) < 1400, len(text)
+    assert set(s) == {"config2_fixed_list", "config3_plain_range", "config4_batched_vs_plain", "config5_serving"}
+    assert s["config4_batched_vs_plain"]["target_1p5x_met"] is False
+    assert s["config5_serving"]["p99_ms"] == 168.0
