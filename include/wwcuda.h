@@ -245,8 +245,8 @@ int ww_batch_tune(ww_ctx *ctx, const ww_unit *sample, uint32_t n, ww_batch_cfg *
  * memory up front and forbid later allocations, or latency-bound loops
  * that cannot afford an allocation's device-wide synchronisation, get the
  * same per-range results as ww_batch_run without any allocation: the
- * scratch lives in one fixed __device__ array of the library (about 450 KB
- * per device, kept until exit).  units: host array, n <= 4096 ranges;
+ * scratch lives in one fixed __device__ array of the library (480 KiB per
+ * device, kept until exit).  units: host array, n <= 4096 ranges;
  * out[n], hits[hit_cap] (at most 4096 records), hit_unit[hit_cap] (may be
  * NULL) and *hit_count are device memory; work is queued on `stream` (a
  * cudaStream_t) and the call does not wait for it.  Calls share the array:

@@ -1,9 +1,9 @@
 """Regenerate the golden fixtures in this folder from the reference's own CPU
 code (oracle/_ref/libwwref.so, compiled in place from the reference tree by
-oracle/Makefile).  Run from the repository root where the reference sources
-are mounted:
+oracle/Makefile).  Run from the repository root, naming the reference
+source tree (its tests.txt gives the end-to-end vectors):
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF_DIR=<tree> && python tests/golden/make_golden.py <tree>
 
     python tests/golden/make_golden.py --long    # config 3's range, minutes
 
@@ -151,7 +151,9 @@ def main() -> None:
         long_ranges(ref)
         return
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    ref_tree = Path(args[0]) if args else Path("/root/reference")
+    if not args or not (Path(args[0]) / "tests.txt").exists():
+        raise SystemExit("usage: make_golden.py <reference source tree> [--long | --results]")
+    ref_tree = Path(args[0])
     cases = parse_tests_txt(ref_tree / "tests.txt")
     (OUT / "tests_txt.json").write_text(json.dumps(cases, indent=1) + "\n")
     print(cases, flush=True)

@@ -11,7 +11,7 @@ The rows come in bands: WW_DEEP_ROWS_<b>(X) holds the primes with
 the rows below 2^b, so a build that sieves to 2^B compiles only the bands up
 to B.
 
-Run from the repository root:  python wwocl-boinc_b200/csrc/gen_deep_table.py
+The build (wwocl-boinc_b200/Makefile) runs it; the header is not committed.
 """
 from pathlib import Path
 

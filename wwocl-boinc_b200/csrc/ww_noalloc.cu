@@ -51,8 +51,9 @@ struct NoAllocScratch {
     u32 hit_unit[kNoAllocMaxHits];
 };
 
-// The scratch of every call on a device (about 450 KB per device that loads
-// the library, held until the process exits).
+// The scratch of every call on a device: 491 552 bytes (480 KiB) per device
+// that loads the library, held until the process exits.
+static_assert(sizeof(NoAllocScratch) == 491552, "the documented scratch size");
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
 struct DeviceSetup {
@@ -65,7 +66,9 @@ DeviceSetup g_setup[kNoAllocMaxDevices];
 std::mutex g_mutex;  // guards g_setup and the host staging below
 
 // Host staging of the per-range state and tile table (copied into the
-// device array on the caller's stream).
+// device array on the caller's stream).  These are pageable: a host-to-device
+// cudaMemcpyAsync from pageable memory returns only once the source has been
+// staged, so the next call may refill them as soon as the mutex is free.
 UnitState g_h_units[kNoAllocMaxUnits];
 u64 g_h_first[kNoAllocMaxUnits + 1];
 
