@@ -5,7 +5,8 @@ source tree (its tests.txt gives the end-to-end vectors):
 
     make -C oracle REF_DIR=<tree> && python tests/golden/make_golden.py <tree>
 
-    python tests/golden/make_golden.py --long    # config 3's range, minutes
+    python tests/golden/make_golden.py <tree> --long     # config 3's range, minutes
+    python tests/golden/make_golden.py <tree> --results  # config 1's results file
 
 Outputs (small, committed):
   ref_ranges.json  per-range PRP count, checksum and CPU result count
@@ -13,6 +14,8 @@ Outputs (small, committed):
                    terms and the wwcpu.cpp hit flags for fixed prime samples
   ref_prps.json    PRP-list digests (count, sum, sha256 of the sorted list)
   ref_long.json    config 3's full range (with --long)
+  results_127_5e7.json  the expected results file of `WWocl 127 5e7` (with
+                   --results): line count, sha256, first and last lines
 """
 from __future__ import annotations
 
@@ -144,11 +147,44 @@ def long_ranges(ref: RefCPU) -> None:
     print(out, flush=True)
 
 
+def results_file(ref: RefCPU, o: Oracle) -> None:
+    """The results file the reference program writes for `WWocl 127 5e7`
+    (config 1): one flush at the range's end (main.cpp:1743-1760), hits
+    sorted by p with the Wieferich kernel's hit first for equal p
+    (main.cpp:843-854, a stable sort of the Wieferich-then-WSS hit list),
+    PRP-only hits dropped (isPrime, main.cpp:869-911), then the checksum line
+    (main.cpp:1759-1766).  Which primes hit is pinned to the reference's own
+    wieferichCPU / wallsunsunCPU flags over every PRP of the range; the hit
+    records' rem/quot and the line formats come from the oracle's
+    restatement (the formats are pinned by tests.txt)."""
+    lo, hi = 127, 50_000_000
+    prps = ref.prp_list(lo, hi, cap=4_000_000)
+    _, _, w_hit, s_hit = ref.list_terms(prps)
+    summ, _, hits = o.scan_range(lo, hi, hit_cap=16384)
+    assert summ["gpu_results"] == len(hits)
+    assert {p for p, r, _, _ in hits if r == 1093} == {int(p) for p, h in zip(prps, w_hit) if h}
+    assert {p for p, r, _, _ in hits if r in (1, 2)} == {int(p) for p, h in zip(prps, s_hit) if h}
+    rc, text, dropped = o.format_results(hits)
+    assert rc >= 0
+    text += "%016X\n" % summ["checksum"]
+    lines = text.splitlines()
+    out = {"start": "127", "end": "5e7", "lo": lo, "hi": hi, "prp_count": int(prps.size),
+           "hit_records": len(hits), "dropped_prp_only": dropped, "lines": len(lines),
+           "wieferich_lines": sum(" Wieferich " in ln for ln in lines),
+           "wallsunsun_lines": sum(" WallSunSun " in ln for ln in lines),
+           "sha256": hashlib.sha256(text.encode()).hexdigest(), "head": lines[:6], "tail": lines[-6:]}
+    (OUT / "results_127_5e7.json").write_text(json.dumps(out, indent=1) + "\n")
+    print({k: v for k, v in out.items() if k not in ("head", "tail")}, flush=True)
+
+
 def main() -> None:
     ref = RefCPU()
     o = Oracle()
     if "--long" in sys.argv:
         long_ranges(ref)
+        return
+    if "--results" in sys.argv:
+        results_file(ref, o)
         return
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     if not args or not (Path(args[0]) / "tests.txt").exists():

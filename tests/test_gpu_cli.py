@@ -30,6 +30,35 @@ def test_tests_txt_vector(tests_txt, tmp_path, case):
     assert f"Checksum: {c['checksum']}" in r.stdout
 
 
+def test_results_file_config1_byte_for_byte(oracle, tmp_path):
+    """`WWocl 127 5e7` (config 1) writes the reference's results file byte
+    for byte: 3890 hit lines sorted by p (the Wieferich line first where one
+    prime has both), then the checksum.  The file is compared with the
+    oracle's restatement of getResults over the oracle's hits and with the
+    committed digest of the file generated from the reference's own CPU hit
+    flags (tests/golden/results_127_5e7.json).  No range below 2e9 has a hit
+    on a pseudoprime, so the dropped count is 0 here; the drop rule itself is
+    tested on the host (test_format_hits_matches_oracle)."""
+    import hashlib
+    import json
+
+    from conftest import GOLDEN
+
+    g = json.loads((GOLDEN / "results_127_5e7.json").read_text())
+    r = run([g["start"], g["end"], "-debug"], tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    got = (tmp_path / "results-WW.txt").read_bytes()
+    summ, _, hits = oracle.scan_range(g["lo"], g["hi"], hit_cap=16384)
+    rc, text, dropped = oracle.format_results(hits)
+    want = (text + "%016X\n" % summ["checksum"]).encode()
+    assert got == want
+    assert hashlib.sha256(got).hexdigest() == g["sha256"]
+    lines = got.decode().splitlines()
+    assert len(lines) == g["lines"] and lines[:6] == g["head"] and lines[-6:] == g["tail"]
+    assert f"Number of results:                 {g['hit_records']}" in r.stdout
+    assert f"PRPs removed from results:         {g['dropped_prp_only']}" in r.stdout
+
+
 def test_separate_kernels_and_ckpt_cadence(tests_txt, tmp_path):
     c = tests_txt[2]  # the Wieferich special instance window
     r = run([c["start"], c["end"], "-separate", "-ckpt", "2e9", "-results", "results-WWocl.txt"], tmp_path)

@@ -155,3 +155,44 @@ def test_calls_out_of_order_are_refused(ww, ctx):
     assert r["id"] == 42 and len(srv.prps(42, r["prps_stored"])) == r["prp_count"]
     srv.close()
     srv.close()
+
+
+def test_requests_admitted_mid_flight_equal_alone_and_oracle(ww, ctx, oracle):
+    """Continuous batching: requests are submitted between steps while
+    others are on the device (widths across two decades, 1e5 to 1e7, plus
+    the known Wieferich and WSS windows).  Every finished request equals its
+    run alone through the context API and the oracle: checksum, PRP count,
+    hit records and PRP list."""
+    units = ww.uneven_units(29, 30, wmin=1e5, wmax=1e7, smin=10**12, smax=2**64 - 10**8)
+    reqs = [(5000 + i, a, b) for i, (a, b) in enumerate(units)]
+    reqs.insert(7, (4998, 2276306935816523 - 5000, 2276306935816523 + 5000))
+    reqs.insert(15, (4999, 338772621946054253 - 5000, 338772621946054253 + 5000))
+    srv = ww.Server(ctx, prp_pool_bytes=1 << 28, max_active=8, epoch_tiles=12, store_prps=True)
+    pending = list(reqs)
+    srv.submit(pending[:5])
+    pending = pending[5:]
+    got, admitted_while_busy, steps = {}, 0, 0
+    while len(got) < len(reqs) and steps < 20000:
+        if pending and steps % 2 == 1:  # two more requests every other step
+            q, active, _ = srv.status()
+            admitted_while_busy += active > 0
+            srv.submit(pending[:2])
+            pending = pending[2:]
+        for r in srv.step():
+            got[r["id"]] = (r, srv.prps(r["id"], r["prps_stored"]), sorted(srv.hits(r["id"])))
+        steps += 1
+    srv.close()
+    assert len(got) == len(reqs)
+    assert admitted_while_busy >= 8  # the submissions really overlapped running requests
+    for rid, a, b in reqs:
+        r, prps, hits = got[rid]
+        alone = ctx.run_range(a, b)
+        want, wprps, whits = oracle.scan_range(a, b, want_prps=True, prp_cap=(b - a) // 2 + 8, hit_cap=10000)
+        assert r["status"] == 0, rid
+        assert (r["checksum"], r["prp_count"], r["hits"]) == \
+               (alone["checksum"], alone["total_prp_count"], alone["result_count"]), rid
+        assert (r["checksum"], r["prp_count"], r["hits"]) == \
+               (want["checksum"], want["prp_count"], want["gpu_results"]), rid
+        assert np.array_equal(np.sort(prps), wprps), rid
+        assert hits == sorted(whits), rid
+    assert got[4998][0]["hits"] >= 1 and got[4999][0]["hits"] >= 1

@@ -4,11 +4,12 @@
 from __future__ import annotations
 
 import hashlib
+import json
 
 import numpy as np
 import pytest
 
-from conftest import sample_names
+from conftest import GOLDEN, sample_names
 
 
 def test_known_answer_wieferich(oracle):
@@ -158,3 +159,19 @@ def test_oracle_matches_reference_code_on_random_ranges(oracle):
         theirs = ref.scan_range(lo, hi)
         assert (mine["prp_count"], mine["checksum"], mine["cpu_results"]) == \
                (theirs["prp_count"], theirs["checksum"], theirs["cpu_results"]), (lo, hi)
+
+
+def test_oracle_results_file_config1_matches_reference_digest(oracle):
+    """The oracle's restatement of getResults over its own hits of
+    [127, 5e7) gives the results file whose digest make_golden.py --results
+    computed after checking the hit set against the reference's own CPU hit
+    flags (wieferichCPU / wallsunsunCPU over every PRP of the range)."""
+    g = json.loads((GOLDEN / "results_127_5e7.json").read_text())
+    summ, _, hits = oracle.scan_range(g["lo"], g["hi"], hit_cap=16384)
+    assert summ["prp_count"] == g["prp_count"] and len(hits) == g["hit_records"]
+    rc, text, dropped = oracle.format_results(hits)
+    text += "%016X\n" % summ["checksum"]
+    assert rc >= 0 and dropped == g["dropped_prp_only"]
+    assert hashlib.sha256(text.encode()).hexdigest() == g["sha256"]
+    lines = text.splitlines()
+    assert lines[:6] == g["head"] and lines[-6:] == g["tail"]
