@@ -152,6 +152,19 @@ int ww_clear_segment(ww_ctx *ctx); /* clearn */
 
 /* getsegprimes over [kernel_start, stop) into the context's PRP buffers. */
 int ww_sieve_prp(ww_ctx *ctx, uint64_t kernel_start, uint64_t stop, int32_t wheel_idx);
+
+/* Sieve depth of the context's sieve launches (ww_sieve_prp, ww_count_prps).
+ * No reference counterpart: getsegprimes sieves by 3..113 only
+ * (getsegprimes.cl:169-225).  After 3..113 every launch sieves by the primes
+ * below 2^20 segment by segment; at depth bits > 20, a launch of 2^26
+ * numbers or more also marks the multiples of the primes below 2^bits, once
+ * per launch (bits <= 30; the first use of a depth on a device builds its
+ * prime table).  Only composites that can never be base-2 pseudoprimes are
+ * marked, so the PRP list is the same at every depth.  A new context sieves
+ * at depth 26; depth 20 turns the large primes off.  The kernel-shaped
+ * ww_launch_getsegprimes, which gets no scratch, always sieves at depth 20. */
+int ww_set_sieve_depth(ww_ctx *ctx, int bits);
+int ww_get_sieve_depth(ww_ctx *ctx, int *bits);
 int ww_wieferich(ww_ctx *ctx);
 int ww_wallsunsun(ww_ctx *ctx);
 int ww_test_prps(ww_ctx *ctx); /* fused wieferich + wallsunsun */

@@ -62,6 +62,45 @@ def test_sieve_prp_sets_match_reference(ctx, ref_prps):
         assert _digest(lst) == (r["count"], r["sum_mod_2_64"], r["sha256"]), name
 
 
+@pytest.mark.parametrize("lo,width", [(127, 1 << 28), (2**20 - 1001, 1 << 27), (2**32 - 2**26 + 1, 1 << 27),
+                                      (2**63 - 2**26 + 7, (1 << 27) + 12345), (2**64 - 2**28 - 1, 1 << 28)])
+def test_sieve_depth_keeps_the_prp_set(ww, lo, width):
+    """The large deep primes (marked once per launch above 2^20) remove only
+    composites that can never be base-2 pseudoprimes: the PRP list is the
+    same at every depth -- over ranges that hold the deep primes themselves
+    (127 .. 2^28), pseudoprimes with large factors, both sides of 2^32 and
+    2^63, and the end of the domain.  Depth 20 is the path pinned to the
+    reference's fixtures and random ranges."""
+    hi = lo + width
+    with ww.Context(0, max_prps=ww.prp_count_bound(lo, hi), max_hits=15000) as c:
+        digests = {}
+        for bits in (20, 24, 26, 28):
+            c.set_sieve_depth(bits)
+            assert c.sieve_depth() == bits
+            c.clear_results()
+            c.clear_segment()
+            c.sieve_prp(lo, hi)
+            c.sync()
+            assert c.counters()["overflow"] == 0
+            digests[bits] = _digest(c.prps())
+        assert len(set(digests.values())) == 1, digests
+        assert c.count_prps(lo, hi) == digests[20][0]  # the counting launch, at depth 28
+
+
+def test_count_prps_depths_agree_to_2p32(ww):
+    """[127, 2^32) holds every deep prime and many base-2 pseudoprimes with a
+    factor above 2^20: its PRP count is the same at depths 20 and 30."""
+    with ww.Context(0, max_prps=1 << 10, max_hits=1024) as c:
+        c.set_sieve_depth(20)
+        n20 = c.count_prps(127, 2**32)
+        c.set_sieve_depth(30)
+        assert c.count_prps(127, 2**32) == n20
+        with pytest.raises(ww.WWError):
+            c.set_sieve_depth(31)
+        with pytest.raises(ww.WWError):
+            c.set_sieve_depth(19)
+
+
 def test_sieve_prp_list_inverse(ww):
     """g_invert holds p^-1 mod 2^64 for each listed p (getsegprimes.cl:291-296)."""
     import torch

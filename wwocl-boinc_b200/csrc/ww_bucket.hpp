@@ -1,0 +1,29 @@
+// ww_bucket.hpp -- the deep sieve's large primes, marked once per launch
+// (ww_bucket.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "ww_deep.cuh"
+
+namespace ww {
+
+// Deepest table: primes below 2^30 (the rows keep r in 32 bits).
+constexpr int kDeepLargeMaxBits = 30;
+
+// Rows of the primes 2^WW_DEEP_BITS < r < 2^bits on one device, in
+// ascending order.
+struct DeepLarge {
+    const DeepRow *rows;
+    u32 n;
+};
+
+// The table for `bits` on the current device, built on first use (a host
+// sieve and one kernel; cached until the process exits).
+int deep_large_device(int bits, DeepLarge *out);
+
+// Zero bits[0, nwords) and mark, for the odd numbers first + 2j (j < nodd),
+// the multiples of the table's primes that the cofactor rule marks.
+int launch_deep_fill(u64 first, u64 nodd, const DeepLarge &t, u32 *bits, u64 nwords, cudaStream_t stream);
+
+}  // namespace ww

@@ -12,8 +12,9 @@
 #include <thread>
 
 #include "../../include/wwcuda.h"
-#include "ww_trace.hpp"
+#include "ww_bucket.hpp"
 #include "ww_kernels.cuh"
+#include "ww_trace.hpp"
 
 using namespace ww;
 
@@ -210,8 +211,10 @@ int with_stream_cursor(void *stream, Launch launch) {
 
 }  // namespace
 
+struct LargeMarks;
 int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime, uint64_t *g_invert,
-                 uint32_t *primecount, uint64_t capacity, uint32_t *overflow, void *stream, u64 *cursor);
+                 uint32_t *primecount, uint64_t capacity, uint32_t *overflow, void *stream, u64 *cursor,
+                 LargeMarks *large = nullptr);
 
 extern "C" {
 
@@ -283,24 +286,56 @@ cudaError_t sieve_slots(int *slots) {
 
 template <class G>
 int launch_sieve_shape(uint64_t low, uint64_t high, uint64_t span, const PrpOut &out, u64 *cursor,
-                       const DeepRow *deep, cudaStream_t stream) {
+                       const DeepRow *deep, cudaStream_t stream, const u32 *marks) {
     const uint64_t per = 2ull * G::kOdd;
     const uint64_t nseg = span / per + (span % per ? 1 : 0);
     int slots = 0;
     WW_CU(sieve_slots<G>(&slots));
     const uint64_t grid = nseg < (uint64_t)slots ? nseg : (uint64_t)slots;
     if (cursor) WW_CU(cudaMemsetAsync(cursor, 0, sizeof(u64), stream));
-    k_sieve_prp<G><<<(unsigned)grid, G::kThreads, G::kSmem, stream>>>(low, high, nseg, out, cursor, deep);
+    k_sieve_prp<G><<<(unsigned)grid, G::kThreads, G::kSmem, stream>>>(low, high, nseg, out, cursor, deep, marks);
     WW_CHECK_LAUNCH();
     return WW_OK;
 }
 
+// One sieve launch over [low, high): the wide shape once the range gives
+// each of its resident CTAs a segment, below that the narrow one, which has
+// twice the segments.
+int launch_sieve_range(uint64_t low, uint64_t high, const PrpOut &out, u64 *cursor, const DeepRow *deep,
+                       cudaStream_t stream, const u32 *marks) {
+    const uint64_t span = high - (low & ~1ull);
+    int wide_slots = 0;
+    WW_CU(sieve_slots<SieveWide>(&wide_slots));
+    const uint64_t wide_segs = span / (2ull * SieveWide::kOdd) + 1;
+    if (wide_segs >= (uint64_t)wide_slots)
+        return launch_sieve_shape<SieveWide>(low, high, span, out, cursor, deep, stream, marks);
+    return launch_sieve_shape<SieveNarrow>(low, high, span, out, cursor, deep, stream, marks);
+}
+
 }  // namespace
 
+// The large deep primes of a context's sieve launches (ww_bucket.cu): the
+// table of the context's depth and the mark bitmap the context owns.
+struct LargeMarks {
+    DeepLarge table;
+    u32 *bits;
+    u64 words;  // capacity of bits
+};
+
+// Launches of at most this many numbers each get one mark bitmap (64 MiB);
+// wider ranges are sieved in pieces of this width.
+constexpr u64 kLargeMarksPiece = 1ull << 30;
+// Below this width a launch sieves with the per-segment deep primes only.
+constexpr u64 kLargeMarksMinSpan = 1ull << 26;
+
 // The sieve launch; with a segment cursor (zeroed here, on the stream) the
-// CTAs take segments dynamically instead of striding.
+// CTAs take segments dynamically instead of striding.  With large (a
+// context's table and bitmap) a launch of kLargeMarksMinSpan numbers or
+// more also marks the multiples of the table's primes: in pieces of
+// kLargeMarksPiece numbers, each a fill kernel and a sieve launch.
 int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime, uint64_t *g_invert,
-                 uint32_t *primecount, uint64_t capacity, uint32_t *overflow, void *stream, u64 *cursor) {
+                 uint32_t *primecount, uint64_t capacity, uint32_t *overflow, void *stream, u64 *cursor,
+                 LargeMarks *large) {
     // g_prime == nullptr: count the PRPs without listing them
     if ((!g_prime && capacity) || !primecount || !overflow) return set_err("null pointer"), WW_ERR_ARG;
     if (low < 127 || high <= low) return set_err("bad range [%llu, %llu)", (unsigned long long)low,
@@ -311,18 +346,26 @@ int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prim
     if (ww_prp_count_bound(low, high) >= 0xffffffffull)
         return set_err("range too wide for a 32-bit PRP counter"), WW_ERR_ARG;
     const uint64_t b0 = low & ~1ull;
-    const uint64_t span = high - b0;
     PrpOut out{(u64 *)g_prime, (u64 *)g_invert, primecount, capacity, overflow};
     const DeepRow *deep = deep_rows_device();
     if (!deep) return WW_ERR_CUDA;
-    // the wide shape once the range gives each of its resident CTAs a
-    // segment; below that the narrow one, which has twice the segments
-    int wide_slots = 0;
-    WW_CU(sieve_slots<SieveWide>(&wide_slots));
-    const uint64_t wide_segs = span / (2ull * SieveWide::kOdd) + 1;
-    if (wide_segs >= (uint64_t)wide_slots)
-        return launch_sieve_shape<SieveWide>(low, high, span, out, cursor, deep, as_stream(stream));
-    return launch_sieve_shape<SieveNarrow>(low, high, span, out, cursor, deep, as_stream(stream));
+    cudaStream_t st = as_stream(stream);
+    if (!large || !large->table.n || high - b0 < kLargeMarksMinSpan)
+        return launch_sieve_range(low, high, out, cursor, deep, st, nullptr);
+    for (u64 a = b0; a < high;) {
+        const u64 b = high - a > kLargeMarksPiece ? a + kLargeMarksPiece : high;
+        const u64 lo = a == b0 ? low : a;  // pieces after the first start on an even number
+        const u64 nodd = (b - a) / 2;
+        // whole segments of the wide shape (2^19 odd numbers) cover either shape's reads
+        const u64 words = ((nodd + SieveWide::kOdd - 1) / SieveWide::kOdd) * (u64)SieveWide::kWords;
+        if (words > large->words) return set_err("mark bitmap too small"), WW_ERR_STATE;
+        int rc = launch_deep_fill(a + 1, nodd, large->table, large->bits, words, st);
+        if (rc) return rc;
+        rc = launch_sieve_range(lo, b, out, cursor, deep, st, large->bits);
+        if (rc) return rc;
+        a = b;
+    }
+    return WW_OK;
 }
 
 extern "C" {
@@ -419,6 +462,13 @@ void destroy_batch_state(BatchState *s);
 void destroy_server_state(ServerState *s);
 }  // namespace ww
 
+// Sieve depth of a new context: the deep primes below 2^kDefaultSieveDepth
+// (ww_set_sieve_depth).
+#ifndef WW_SIEVE_DEPTH
+#define WW_SIEVE_DEPTH 26
+#endif
+constexpr int kDefaultSieveDepth = WW_SIEVE_DEPTH;
+
 struct ww_ctx {
     ww::BatchState *batch = nullptr;
     ww::ServerState *server = nullptr;
@@ -439,10 +489,37 @@ struct ww_ctx {
     u32 *d_count = nullptr;   // ww_count_prps: count, max, overflow
     u64 *d_cursor = nullptr;  // work cursors: [0] ww_test_prps, [1] ww_sieve_prp, [2] ww_wieferich,
                               // [3] ww_wallsunsun, [4] ww_count_prps, [5 + i] host chunk i
+    // the large deep primes of ww_sieve_prp / ww_count_prps (ww_set_sieve_depth)
+    int sieve_depth = kDefaultSieveDepth;
+    LargeMarks large{{nullptr, 0}, nullptr, 0};
 };
 
 namespace {
 constexpr u64 kHostChunksMax = 1024;
+
+// The context's large deep primes for its sieve launches: nullptr at depth
+// WW_DEEP_BITS; otherwise the table of its depth and the context's mark
+// bitmap (allocated on first use, one piece wide).
+int context_large_marks(ww_ctx *c, LargeMarks **out) {
+    *out = nullptr;
+    if (c->sieve_depth <= WW_DEEP_BITS) return WW_OK;
+    DeepLarge t{nullptr, 0};
+    const int rc = deep_large_device(c->sieve_depth, &t);
+    if (rc) return rc;
+    c->large.table = t;
+    if (!c->large.bits) {
+        const u64 words = (kLargeMarksPiece / 2 / SieveWide::kOdd) * (u64)SieveWide::kWords;
+        const cudaError_t e = cudaMalloc(&c->large.bits, words * sizeof(u32));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            c->large.bits = nullptr;
+            return set_err("mark bitmap: %s", cudaGetErrorString(e)), WW_ERR_NOMEM;
+        }
+        c->large.words = words;
+    }
+    *out = &c->large;
+    return WW_OK;
+}
 }
 
 extern "C" {
@@ -489,6 +566,7 @@ void ww_close(ww_ctx *c) {
     cudaFree(c->dc);
     cudaFree(c->d_cursor);
     cudaFree(c->d_count);
+    cudaFree(c->large.bits);
     if (c->hc) cudaFreeHost(c->hc);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     cudaFree(c->d_chunk);
@@ -597,8 +675,26 @@ int ww_clear_segment(ww_ctx *c) {
 int ww_sieve_prp(ww_ctx *c, uint64_t kernel_start, uint64_t stop, int32_t wheel_idx) {
     ww::TraceRange trace("ww_sieve_prp");
     WW_NEED_BUFFERS(c);
+    LargeMarks *large = nullptr;
+    const int rc = context_large_marks(c, &large);
+    if (rc) return rc;
     return launch_sieve(kernel_start, stop, wheel_idx, (uint64_t *)c->prime, (uint64_t *)c->inv, c->dc->primecount,
-                        c->cap, &c->dc->overflow, c->stream, c->d_cursor + 1);
+                        c->cap, &c->dc->overflow, c->stream, c->d_cursor + 1, large);
+}
+
+int ww_set_sieve_depth(ww_ctx *c, int bits) {
+    if (!c) return set_err("null context"), WW_ERR_ARG;
+    if (bits != WW_DEEP_BITS && (bits <= WW_DEEP_BITS || bits > kDeepLargeMaxBits))
+        return set_err("sieve depth %d: %d (no large primes) or %d..%d", bits, WW_DEEP_BITS, WW_DEEP_BITS + 1,
+                       kDeepLargeMaxBits), WW_ERR_ARG;
+    c->sieve_depth = bits;
+    return WW_OK;
+}
+
+int ww_get_sieve_depth(ww_ctx *c, int *bits) {
+    if (!c || !bits) return set_err("null argument"), WW_ERR_ARG;
+    *bits = c->sieve_depth;
+    return WW_OK;
 }
 
 int ww_wieferich(ww_ctx *c) {
@@ -727,8 +823,11 @@ int ww_count_prps(ww_ctx *c, uint64_t lo, uint64_t hi, uint64_t *count) {
         if (ww_find_wheel_offset(&ks, &idx) != WW_OK) break;  // nothing prime to 30 is left below 2^64
         if (ks < b) {
             WW_CU(cudaMemsetAsync(c->d_count, 0, 4 * sizeof(u32), c->stream));
-            const int rc = launch_sieve(ks, b, idx, nullptr, nullptr, c->d_count, 0, c->d_count + 2, c->stream,
-                                        c->d_cursor + 4);
+            LargeMarks *large = nullptr;
+            int rc = context_large_marks(c, &large);
+            if (rc) return rc;
+            rc = launch_sieve(ks, b, idx, nullptr, nullptr, c->d_count, 0, c->d_count + 2, c->stream,
+                              c->d_cursor + 4, large);
             if (rc) return rc;
             u32 n = 0;
             WW_CU(cudaMemcpyAsync(&n, c->d_count, sizeof(u32), cudaMemcpyDeviceToHost, c->stream));

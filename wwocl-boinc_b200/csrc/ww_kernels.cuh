@@ -27,10 +27,13 @@ namespace ww {
 // With a segment cursor (zeroed before the launch) the CTAs take segments
 // one at a time from it; without one (a launch captured into a graph, or
 // one that found every cursor of the library's pool busy) they stride over
-// the segments.
+// the segments.  marks (optional): the large deep primes' marks of the whole
+// launch, bit j of word w = odd number b0 + 2(32 w + j) + 1 (ww_bucket.cu),
+// ORed into each segment's bitmap.
 template <class G>
 __global__ void __launch_bounds__(G::kThreads, 1024 / G::kThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out,
-                                                                              u64 *cursor, const DeepRow *deep) {
+                                                                              u64 *cursor, const DeepRow *deep,
+                                                                              const u32 *__restrict__ marks) {
     extern __shared__ u32 sieve_smem[];  // G::kSmem bytes
     u32 *bitmap = sieve_smem;
     u32(*queue)[kQueueCap] = reinterpret_cast<u32(*)[kQueueCap]>(sieve_smem + G::kWords);
@@ -56,12 +59,13 @@ __global__ void __launch_bounds__(G::kThreads, 1024 / G::kThreads) k_sieve_prp(u
         {
             const int w0 = threadIdx.x * G::kWordsPerThread;
             const u64 n0 = b0 + seg_off + 64ull * (u64)w0 + 1;  // may wrap past 2^64 beyond hi
+            const u32 *seg_marks = marks ? marks + seg * (u64)G::kWords : nullptr;
 #define WW_J0(R) u32 j##R = first_hit<R>(n0);
             WW_FOR_SMALL_PRIMES(WW_J0)
 #undef WW_J0
 #pragma unroll 4
             for (int w = w0; w < w0 + G::kWordsPerThread; ++w) {
-                u32 m = 0;
+                u32 m = seg_marks ? seg_marks[w] : 0u;
 #define WW_MASK(R) m |= prime_mask<R>(j##R); step_hit<R>(j##R);
                 WW_FOR_SMALL_PRIMES(WW_MASK)
 #undef WW_MASK

@@ -109,6 +109,8 @@ _SIGS = {
     "ww_clear_results": (C.c_int, [_VP]),
     "ww_clear_segment": (C.c_int, [_VP]),
     "ww_sieve_prp": (C.c_int, [_VP, C.c_uint64, C.c_uint64, C.c_int32]),
+    "ww_set_sieve_depth": (C.c_int, [_VP, C.c_int]),
+    "ww_get_sieve_depth": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "ww_wieferich": (C.c_int, [_VP]),
     "ww_wallsunsun": (C.c_int, [_VP]),
     "ww_test_prps": (C.c_int, [_VP]),
@@ -327,6 +329,15 @@ class Context:
         if ks >= stop:
             return
         check(_L.ww_sieve_prp(self.h, ks, stop, idx), "ww_sieve_prp")
+
+    def set_sieve_depth(self, bits: int) -> None:
+        """Deep primes below 2^bits in the sieve launches (20: per-segment primes only)."""
+        check(_L.ww_set_sieve_depth(self.h, bits), "ww_set_sieve_depth")
+
+    def sieve_depth(self) -> int:
+        b = C.c_int(0)
+        check(_L.ww_get_sieve_depth(self.h, C.byref(b)), "ww_get_sieve_depth")
+        return b.value
 
     def wieferich(self):
         check(_L.ww_wieferich(self.h), "ww_wieferich")
