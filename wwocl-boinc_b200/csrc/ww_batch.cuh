@@ -39,10 +39,12 @@ struct BatchArgs {
     const u64 *tile_first;
     u64 n_tiles;
     u64 *next_tile;          // queue head
-    // round-robin over active units (serving): at most `budget` tiles this launch
-    u32 *rr;
+    // serving: at most `budget` tiles this launch, handed out in the order of
+    // `order` (slot indices, earliest deadline first; n_order entries)
     u32 *epoch_tiles;
     u32 budget;
+    const u32 *order;
+    u32 n_order;
     // hits: p, result, rem, quot, unit
     u64 *hit_p;
     int *hit_result, *hit_rem, *hit_quot;
@@ -132,9 +134,10 @@ constexpr size_t batch_smem_bytes() {
 }
 
 // Hand out the next tile.  Batch: the global queue head over the static
-// tile table.  Serving: round-robin over the units, each unit's own cursor,
-// at most `budget` tiles per launch; every loop is bounded by the number of
-// units, so an exhausted queue ends the kernel instead of spinning.
+// tile table.  Serving: the first unit in the host's priority order that
+// has tiles left, through that unit's own cursor, at most `budget` tiles per
+// launch; the loop is bounded by the number of units, so an exhausted queue
+// ends the kernel instead of spinning.
 template <bool SERVE>
 __device__ __forceinline__ bool next_tile(const BatchArgs &a, u32 &unit, u64 &tile) {
     if (!SERVE) {
@@ -150,10 +153,12 @@ __device__ __forceinline__ bool next_tile(const BatchArgs &a, u32 &unit, u64 &ti
         return true;
     }
     if (atomicAdd(a.epoch_tiles, 1u) >= a.budget) return false;
-    for (u32 tries = 0; tries < a.n_units; ++tries) {
-        const u32 k = atomicAdd(a.rr, 1u) % a.n_units;
+    for (u32 i = 0; i < a.n_order; ++i) {
+        const u32 k = a.order[i];
         UnitState &u = a.units[k];
-        if (!u.active || u.next_tile >= u.n_tiles) continue;
+        // the cursor is read past L1 (other CTAs move it); a stale value
+        // only costs an atomic that finds the unit exhausted
+        if (!u.active || *(volatile u64 *)&u.next_tile >= u.n_tiles) continue;
         const u64 t = atomicAdd((unsigned long long *)&u.next_tile, 1ull);
         if (t < u.n_tiles) {
             unit = k;

@@ -45,7 +45,7 @@ struct NoAllocScratch {
     UnitState units[kNoAllocMaxUnits];
     u64 tile_first[kNoAllocMaxUnits + 1];
     u64 next_tile;
-    u32 rr, epoch, hit_count, overflow;
+    u32 reserved, epoch, hit_count, overflow;
     u64 hit_p[kNoAllocMaxHits];
     int hit_result[kNoAllocMaxHits], hit_rem[kNoAllocMaxHits], hit_quot[kNoAllocMaxHits];
     u32 hit_unit[kNoAllocMaxHits];
@@ -181,7 +181,6 @@ extern "C" int ww_batch_run_noalloc(const ww_unit *units, uint32_t n, ww_unit_re
     a.tile_first = s->tile_first;
     a.n_tiles = acc;
     a.next_tile = &s->next_tile;
-    a.rr = &s->rr;
     a.epoch_tiles = &s->epoch;
     a.hit_p = s->hit_p;
     a.hit_result = s->hit_result;
