@@ -208,8 +208,7 @@ def run_reference(args):
     return 0
 
 
-def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30, chain_peak: float | None = None,
-                       depth: int = 20) -> dict:
+def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30, chain_peak: float | None = None) -> dict:
     """The plain one-range path over [2^64-2^35, 2^64-2^35+width): per 2^30
     numbers (the checkpoint cadence) clear, sieve + SPRP, both tests, sync and
     read the counters back, as the reference program's loop does.  With the
@@ -218,6 +217,7 @@ def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30, chain_pe
     lo = 2**64 - 2**35
     hi = lo + width
     ctx = ww.Context(local, max_prps=ww.prp_count_bound(0, ckpt), max_hits=15000)
+    depth = ctx.sieve_depth()  # deep primes below 2^depth (large ones marked once per launch)
     ctx.run_range(lo, min(hi, lo + ckpt))  # warm
 
     # sieve and test kernel times of one full checkpoint segment
@@ -258,7 +258,7 @@ def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30, chain_pe
            "segment_2p30": {"prps": seg_prps, "sieve_ms": sieve_ms, "test_ms": test_ms,
                             "sieve_numbers_per_s": min(width, ckpt) / (sieve_ms * 1e-3),
                             "test_primes_per_s": seg_prps / (test_ms * 1e-3)},
-           "checksum": "%016X" % cks, "results": res}
+           "checksum": "%016X" % cks, "results": res, "sieve_depth": depth}
     if chain_peak:
         # end to end over sieve + tests, in the same 32-bit multiply units as
         # the test kernel's roofline (k = 64 here): the reference's SPRP of a
