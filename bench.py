@@ -61,7 +61,7 @@ def parse_args():
     ap.add_argument("--range-width", type=float, default=float(1 << 34),
                     help="width of the plain-path range leg starting at 2^64-2^35 (0: skip)")
     ap.add_argument("--batch-config", default="",
-                    help="force the batched configuration SEG_WORDS/THREADS/PPT instead of the autotuner's choice")
+                    help="force the batched configuration SEG_WORDS/THREADS/PPT[/JOINT] instead of the autotuner's choice")
     ap.add_argument("--batch-units", type=int, default=4096,
                     help="units of the seed-11 uneven mix for the batched-vs-plain leg (4096: the whole mix; 0: skip)")
     ap.add_argument("--serve-seconds", type=float, default=120.0,
@@ -357,7 +357,7 @@ def compare_batched_plain(ww, local: int, units: list, workload: str, tune_units
             "plain_fused": {"units": nf, "primes_per_s": fused_prps / fused_s if nf else None,
                             "definition": "per range: sieve, fused Wieferich+WSS kernel, read-back"},
             "tuned_config": {"seg_words": cfg[0], "seg_bytes": 4 * cfg[0], "threads": cfg[1],
-                             "primes_per_thread": cfg[2]}}
+                             "primes_per_thread": cfg[2], "joint_test_loop": cfg[3]}}
 
 
 def compare_batched_per_run(ww, local: int, units: list, workload: str) -> dict:
@@ -506,7 +506,8 @@ def summarize(line: dict, extra: dict) -> dict:
             "target_1p5x_met": g["target_1p5x_met"], "per_unit_bit_identical": g["per_unit_bit_identical"],
             "narrow_ratio": r(g["narrow_units"]["speedup_batched_vs_plain"]),
             "per_process_ratio_note": r(g["per_run"].get("speedup_batched_vs_per_run")),
-            "tuned": "%d/%d/%d" % tuple(g["tuned_config"][k] for k in ("seg_words", "threads", "primes_per_thread"))}
+            "tuned": "%d/%d/%d/%d" % tuple(g["tuned_config"][k] for k in ("seg_words", "threads", "primes_per_thread",
+                                                                           "joint_test_loop"))}
     if "serving" in extra:
         g = extra["serving"]
         out["config5_serving"] = {"requests": g["requests"], "p50_ms": r(g["p50_ms"]), "p99_ms": r(g["p99_ms"]),

@@ -234,9 +234,11 @@ typedef struct {
 } ww_unit_result;
 
 /* seg_words: 32-bit words of a tile's bitmap (64 integers per word);
- * threads: per CTA; ppt: primes per thread in the test phase. */
+ * threads: per CTA; ppt: primes per thread in the test phase (batches of 32
+ * PRPs a warp collects before testing); joint: 1 = the Wieferich and WSS
+ * tests of a prime in one loop, 0 = one after the other. */
 typedef struct {
-    uint32_t seg_words, threads, ppt, reserved;
+    uint32_t seg_words, threads, ppt, joint;
 } ww_batch_cfg;
 
 int ww_batch_configs(ww_batch_cfg *out, uint32_t cap, uint32_t *n);

@@ -70,7 +70,8 @@ def test_summary_is_short_and_carries_every_leg():
                                   "speedup_batched_vs_plain": 1.04, "target_1p5x_met": False,
                                   "per_unit_bit_identical": True, "narrow_units": {"speedup_batched_vs_plain": 2.6},
                                   "per_run": {"speedup_batched_vs_per_run": 60.0},
-                                  "tuned_config": {"seg_words": 16384, "threads": 512, "primes_per_thread": 1}},
+                                  "tuned_config": {"seg_words": 16384, "threads": 512, "primes_per_thread": 1,
+                                                   "joint_test_loop": 0}},
              "serving": {"requests": 24008, "p50_ms": 15.9, "p99_ms": 168.0, "max_ms": 394.0, "primes_per_s": 5.1e8,
                          "all_ok": True, "cpu_checksum_equal_on_smallest": True}}
     s = bench.summarize(line, extra)

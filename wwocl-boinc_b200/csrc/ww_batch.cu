@@ -46,33 +46,42 @@ namespace {
 typedef void (*TileKernel)(BatchArgs);
 
 struct CfgEntry {
-    int seg_words, threads, ppt;
+    int seg_words, threads, ppt, joint;
     TileKernel kernel;        // static tile table (batch)
     TileKernel serve_kernel;  // round-robin over request slots (serving)
     size_t smem;
 };
 
-template <int W, int T, int P>
+template <int W, int T, int P, int J = 0>
 CfgEntry entry() {
-    typedef BatchCfg<W, T, P> C;
-    return CfgEntry{W, T, P, &k_tiles<C, false>, &k_tiles<C, true>, batch_smem_bytes<C>()};
+    typedef BatchCfg<W, T, P, J> C;
+    return CfgEntry{W, T, P, J, &k_tiles<C, false>, &k_tiles<C, true>, batch_smem_bytes<C>()};
 }
 
-// Segment bitmaps of 16-128 KB (the whole segment must sit in one CTA's
-// shared memory, at most 227 KB), 128-1024 threads, 1-2 primes per thread.
+// Segment bitmaps of 16-128 KB: the whole segment sits in one CTA's shared
+// memory (at most 227 KB per CTA on the B200, so a 256 KB segment cannot be
+// a tile), beside the warps' queues.  128-1024 threads.  1-8 batches of 32
+// PRPs per warp before testing: 4 and 8 only at 256 threads, where they
+// take 78-79 registers without spilling -- at 512 threads (64 registers)
+// they spill 144 and 268 bytes per thread.  The joint test loop (both
+// tests in one loop, 72 registers in the list kernel) at 256 and 512
+// threads.
 const std::vector<CfgEntry> &configs() {
     static const std::vector<CfgEntry> table = {
-        entry<4096, 128, 1>(),   entry<4096, 256, 1>(),   entry<4096, 512, 1>(),   entry<4096, 256, 2>(),
-        entry<8192, 256, 1>(),   entry<8192, 512, 1>(),   entry<8192, 1024, 1>(),  entry<8192, 256, 2>(),
-        entry<16384, 256, 1>(),  entry<16384, 512, 1>(),  entry<16384, 1024, 1>(), entry<16384, 512, 2>(),
-        entry<32768, 256, 1>(),  entry<32768, 512, 1>(),
+        entry<4096, 128, 1>(),     entry<4096, 256, 1>(),     entry<4096, 512, 1>(),    entry<4096, 256, 2>(),
+        entry<8192, 256, 1>(),     entry<8192, 512, 1>(),     entry<8192, 1024, 1>(),   entry<8192, 256, 2>(),
+        entry<8192, 256, 4>(),     entry<8192, 256, 8>(),     entry<16384, 256, 1>(),   entry<16384, 512, 1>(),
+        entry<16384, 1024, 1>(),   entry<16384, 512, 2>(),    entry<32768, 256, 1>(),   entry<32768, 512, 1>(),
+        entry<8192, 256, 1, 1>(),  entry<16384, 256, 1, 1>(), entry<16384, 512, 1, 1>(),
     };
     return table;
 }
 
 const CfgEntry *find_cfg(const ww_batch_cfg &c) {
     for (const CfgEntry &e : configs())
-        if (e.seg_words == (int)c.seg_words && e.threads == (int)c.threads && e.ppt == (int)c.ppt) return &e;
+        if (e.seg_words == (int)c.seg_words && e.threads == (int)c.threads && e.ppt == (int)c.ppt &&
+            e.joint == (int)c.joint)
+            return &e;
     return nullptr;
 }
 
@@ -273,7 +282,8 @@ int ww_batch_configs(ww_batch_cfg *out, uint32_t cap, uint32_t *n) {
     const auto &t = configs();
     *n = (uint32_t)t.size();
     for (uint32_t i = 0; i < cap && i < t.size(); ++i)
-        out[i] = ww_batch_cfg{(uint32_t)t[i].seg_words, (uint32_t)t[i].threads, (uint32_t)t[i].ppt, 0};
+        out[i] = ww_batch_cfg{(uint32_t)t[i].seg_words, (uint32_t)t[i].threads, (uint32_t)t[i].ppt,
+                              (uint32_t)t[i].joint};
     return WW_OK;
 }
 
@@ -402,7 +412,7 @@ int ww_batch_tune(ww_ctx *ctx, const ww_unit *sample, uint32_t n, ww_batch_cfg *
         cudaEventElapsedTime(&ms, a, b);
         if (ms < bestv) {
             bestv = ms;
-            bestc = ww_batch_cfg{(uint32_t)e.seg_words, (uint32_t)e.threads, (uint32_t)e.ppt, 0};
+            bestc = ww_batch_cfg{(uint32_t)e.seg_words, (uint32_t)e.threads, (uint32_t)e.ppt, (uint32_t)e.joint};
         }
     }
     cudaEventDestroy(a);

@@ -55,12 +55,20 @@ struct BatchArgs {
     const DeepRow *deep;     // the deep-sieve table (deep_rows_device())
 };
 
-template <int SEG_WORDS, int THREADS, int PPT>
+// A tile configuration: SEG_WORDS bitmap words, THREADS per CTA, PPT batches
+// of 32 PRPs a warp collects before testing them, and JOINT = 1 for the
+// Wieferich and WSS tests of a prime in one loop (the list kernel's form)
+// instead of one after the other.
+template <int SEG_WORDS, int THREADS, int PPT, int JOINT = 0>
 struct BatchCfg {
     static constexpr int kWords = SEG_WORDS;
     static constexpr int kThreads = THREADS;
     static constexpr int kWarps = THREADS / 32;
     static constexpr int kPpt = PPT;
+    static constexpr bool kJoint = JOINT != 0;
+    // joint configurations are held to 1024 threads per SM (64 registers);
+    // the others take what the compiler chooses
+    static constexpr int kMinBlocks = JOINT ? 1024 / THREADS : 1;
     static constexpr int kChunks = SEG_WORDS / 32;
     static constexpr u64 kTileNumbers = 64ull * SEG_WORDS;  // integers per tile
     static constexpr int kCandCap = 416;  // as kQueueCap: 31 carried + at most 378 per 32-word chunk
@@ -89,7 +97,7 @@ __device__ __forceinline__ void emit_batch_hit(const BatchArgs &a, u32 unit, u64
 
 // Wieferich + WSS on the warp's PRP queue entries [base, base + 32*PPT);
 // `valid` lanes only.  Adds to the warp's accumulator (lane 0 holds it).
-template <int PPT>
+template <int PPT, bool JOINT>
 __device__ __forceinline__ void test_batch(const u64 *qp, int n_valid, u32 unit, const BatchArgs &a,
                                            WarpAcc &acc) {
     const int lane = threadIdx.x & 31;
@@ -102,12 +110,16 @@ __device__ __forceinline__ void test_batch(const u64 *qp, int n_valid, u32 unit,
         const u64 p = act ? qp[idx] : 0xFFFFFFFFFFFFFFC5ull;  // 2^64-59, a harmless prime
         const u64 q = inv64(p);
         const D2 one = m2_one(p);
-        // the two tests one after the other rather than in one joint loop:
-        // fewer registers live at once, so the 512-thread tiles fit 64
-        // registers (two CTAs, 32 warps per SM) -- measured faster here,
-        // while the list kernel keeps the joint loop
-        const D2 s = wieferich_digits(p, q, one);
-        const D2 c = wss_digits(p, q, one);
+        // one after the other: fewer registers live at once, so the
+        // 512-thread tiles fit 64 registers (two CTAs, 32 warps per SM);
+        // the joint loop has three independent squarings per step
+        D2 s, c;
+        if (JOINT) {
+            both_digits(p, q, one, s, c);
+        } else {
+            s = wieferich_digits(p, q, one);
+            c = wss_digits(p, q, one);
+        }
         if (act) {
             sum += (s.d1 & 0xffffffffull) + (c.d1 & 0xffffffffull);
             ++cnt;
@@ -170,7 +182,7 @@ __device__ __forceinline__ bool next_tile(const BatchArgs &a, u32 &unit, u64 &ti
 }
 
 template <class Cfg, bool SERVE>
-__global__ void __launch_bounds__(Cfg::kThreads) k_tiles(BatchArgs a) {
+__global__ void __launch_bounds__(Cfg::kThreads, Cfg::kMinBlocks) k_tiles(BatchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     u64(*prpq)[Cfg::kPrpCap] = reinterpret_cast<u64(*)[Cfg::kPrpCap]>(smem);
     u32 *bitmap = reinterpret_cast<u32 *>(smem + (size_t)Cfg::kWarps * Cfg::kPrpCap * 8);
@@ -262,7 +274,7 @@ __global__ void __launch_bounds__(Cfg::kThreads) k_tiles(BatchArgs a) {
             __syncwarp();
             while (pn >= 32 * Cfg::kPpt) {
                 pn -= 32 * Cfg::kPpt;
-                test_batch<Cfg::kPpt>(pq + pn, 32 * Cfg::kPpt, unit, a, acc);
+                test_batch<Cfg::kPpt, Cfg::kJoint>(pq + pn, 32 * Cfg::kPpt, unit, a, acc);
                 __syncwarp();
             }
         };
@@ -303,7 +315,7 @@ __global__ void __launch_bounds__(Cfg::kThreads) k_tiles(BatchArgs a) {
             if (!more) break;
         }
         if (pn > 0) {
-            test_batch<Cfg::kPpt>(pq, pn, unit, a, acc);
+            test_batch<Cfg::kPpt, Cfg::kJoint>(pq, pn, unit, a, acc);
             pn = 0;
         }
         if (lane == 0 && acc.count) {

@@ -63,10 +63,10 @@ class UnitResult(C.Structure):
 
 class BatchCfg(C.Structure):
     _fields_ = [("seg_words", C.c_uint32), ("threads", C.c_uint32), ("ppt", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("joint", C.c_uint32)]
 
     def as_tuple(self):
-        return (self.seg_words, self.threads, self.ppt)
+        return (self.seg_words, self.threads, self.ppt, self.joint)
 
 
 class Request(C.Structure):
@@ -434,7 +434,7 @@ class Context:
         return c
 
 
-def batch_configs() -> list[tuple[int, int, int]]:
+def batch_configs() -> list[tuple[int, int, int, int]]:
     n = C.c_uint32(0)
     check(_L.ww_batch_configs(None, 0, C.byref(n)), "ww_batch_configs")
     arr = (BatchCfg * n.value)()
@@ -457,16 +457,16 @@ class Batch:
         check(_L.ww_batch_reserve_hits(ctx.h, max_hits), "ww_batch_reserve_hits")
         self.max_hits = max_hits
 
-    def set_config(self, seg_words: int, threads: int, ppt: int) -> None:
-        c = BatchCfg(seg_words, threads, ppt, 0)
+    def set_config(self, seg_words: int, threads: int, ppt: int, joint: int = 0) -> None:
+        c = BatchCfg(seg_words, threads, ppt, joint)
         check(_L.ww_batch_set_config(self.ctx.h, C.byref(c)), "ww_batch_set_config")
 
-    def config(self) -> tuple[int, int, int]:
+    def config(self) -> tuple[int, int, int, int]:
         c = BatchCfg()
         check(_L.ww_batch_get_config(self.ctx.h, C.byref(c)), "ww_batch_get_config")
         return c.as_tuple()
 
-    def tune(self, sample) -> tuple[tuple[int, int, int], float]:
+    def tune(self, sample) -> tuple[tuple[int, int, int, int], float]:
         u = _units(sample)
         best = BatchCfg()
         ms = C.c_float(0)
