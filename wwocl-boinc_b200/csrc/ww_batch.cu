@@ -705,7 +705,7 @@ int ww_server_step(ww_ctx *ctx, ww_request_result *done, uint32_t cap, uint32_t 
     // ---- one epoch over every admitted request, tiles handed out earliest
     // deadline first: a request's deadline is its submission time plus twice
     // the time its tiles take on the whole GPU (a bounded slowdown for every
-    // size).  In a simulation of the 200 req/s stream this took the p99
+    // size).  In a model of the 200 req/s stream (serve_sim.py) this took the p99
     // latency from 134 ms (equal round-robin shares) to 93 ms at the same
     // p50.  Until a step has been timed, the order is that of submission.
     const double wave_s = s.tile_s > 0 ? s.tile_s : 1e-6;
