@@ -165,6 +165,15 @@ int ww_sieve_prp(ww_ctx *ctx, uint64_t kernel_start, uint64_t stop, int32_t whee
  * ww_launch_getsegprimes, which gets no scratch, always sieves at depth 20. */
 int ww_set_sieve_depth(ww_ctx *ctx, int bits);
 int ww_get_sieve_depth(ww_ctx *ctx, int *bits);
+
+/* Segment shape of the context's sieve launches (no reference counterpart;
+ * with the depth, what the program's autotune picks in place of the
+ * reference's work-size profiling, main.cpp:959-1107): 1 = segments of 2^20
+ * numbers for 512-thread CTAs, 2 = 2^19 numbers for 256-thread CTAs, 0 (the
+ * default) = the wide shape when the launch gives each resident CTA a
+ * segment, else the narrow one.  Results do not depend on the shape. */
+int ww_set_sieve_shape(ww_ctx *ctx, int shape);
+int ww_get_sieve_shape(ww_ctx *ctx, int *shape);
 int ww_wieferich(ww_ctx *ctx);
 int ww_wallsunsun(ww_ctx *ctx);
 int ww_test_prps(ww_ctx *ctx); /* fused wieferich + wallsunsun */

@@ -87,6 +87,23 @@ def test_sieve_depth_keeps_the_prp_set(ww, lo, width):
         assert c.count_prps(lo, hi) == digests[20][0]  # the counting launch, at depth 28
 
 
+def test_sieve_shapes_give_the_same_prp_set(ww, ref_prps):
+    """Both segment shapes of the context's sieve (2^20 numbers for 512
+    threads, 2^19 for 256) give the reference's PRP sets."""
+    with ww.Context(0, max_prps=1 << 22, max_hits=15000) as c:
+        for shape in (1, 2, 0):
+            c.set_sieve_shape(shape)
+            assert c.sieve_shape() == shape
+            for name, r in ref_prps.items():
+                c.clear_results()
+                c.clear_segment()
+                c.sieve_prp(r["lo"], r["hi"])
+                c.sync()
+                assert _digest(c.prps()) == (r["count"], r["sum_mod_2_64"], r["sha256"]), (shape, name)
+        with pytest.raises(ww.WWError):
+            c.set_sieve_shape(3)
+
+
 def test_count_prps_depths_agree_to_2p32(ww):
     """[127, 2^32) holds every deep prime and many base-2 pseudoprimes with a
     factor above 2^20: its PRP count is the same at depths 20 and 30."""

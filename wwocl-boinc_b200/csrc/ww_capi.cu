@@ -214,7 +214,7 @@ int with_stream_cursor(void *stream, Launch launch) {
 struct LargeMarks;
 int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime, uint64_t *g_invert,
                  uint32_t *primecount, uint64_t capacity, uint32_t *overflow, void *stream, u64 *cursor,
-                 LargeMarks *large = nullptr);
+                 LargeMarks *large = nullptr, int shape = 0);
 
 extern "C" {
 
@@ -298,16 +298,16 @@ int launch_sieve_shape(uint64_t low, uint64_t high, uint64_t span, const PrpOut 
     return WW_OK;
 }
 
-// One sieve launch over [low, high): the wide shape once the range gives
-// each of its resident CTAs a segment, below that the narrow one, which has
-// twice the segments.
+// One sieve launch over [low, high).  shape 1: the wide segments, 2: the
+// narrow ones, 0: the wide shape once the range gives each of its resident
+// CTAs a segment, below that the narrow one, which has twice the segments.
 int launch_sieve_range(uint64_t low, uint64_t high, const PrpOut &out, u64 *cursor, const DeepRow *deep,
-                       cudaStream_t stream, const u32 *marks) {
+                       cudaStream_t stream, const u32 *marks, int shape) {
     const uint64_t span = high - (low & ~1ull);
     int wide_slots = 0;
     WW_CU(sieve_slots<SieveWide>(&wide_slots));
     const uint64_t wide_segs = span / (2ull * SieveWide::kOdd) + 1;
-    if (wide_segs >= (uint64_t)wide_slots)
+    if (shape == 1 || (shape == 0 && wide_segs >= (uint64_t)wide_slots))
         return launch_sieve_shape<SieveWide>(low, high, span, out, cursor, deep, stream, marks);
     return launch_sieve_shape<SieveNarrow>(low, high, span, out, cursor, deep, stream, marks);
 }
@@ -335,7 +335,7 @@ constexpr u64 kLargeMarksMinSpan = 1ull << 26;
 // kLargeMarksPiece numbers, each a fill kernel and a sieve launch.
 int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prime, uint64_t *g_invert,
                  uint32_t *primecount, uint64_t capacity, uint32_t *overflow, void *stream, u64 *cursor,
-                 LargeMarks *large) {
+                 LargeMarks *large, int shape) {
     // g_prime == nullptr: count the PRPs without listing them
     if ((!g_prime && capacity) || !primecount || !overflow) return set_err("null pointer"), WW_ERR_ARG;
     if (low < 127 || high <= low) return set_err("bad range [%llu, %llu)", (unsigned long long)low,
@@ -351,7 +351,7 @@ int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prim
     if (!deep) return WW_ERR_CUDA;
     cudaStream_t st = as_stream(stream);
     if (!large || !large->table.n || high - b0 < kLargeMarksMinSpan)
-        return launch_sieve_range(low, high, out, cursor, deep, st, nullptr);
+        return launch_sieve_range(low, high, out, cursor, deep, st, nullptr, shape);
     for (u64 a = b0; a < high;) {
         const u64 b = high - a > kLargeMarksPiece ? a + kLargeMarksPiece : high;
         const u64 lo = a == b0 ? low : a;  // pieces after the first start on an even number
@@ -361,7 +361,7 @@ int launch_sieve(uint64_t low, uint64_t high, int32_t wheelidx, uint64_t *g_prim
         if (words > large->words) return set_err("mark bitmap too small"), WW_ERR_STATE;
         int rc = launch_deep_fill(a + 1, nodd, large->table, large->bits, words, st);
         if (rc) return rc;
-        rc = launch_sieve_range(lo, b, out, cursor, deep, st, large->bits);
+        rc = launch_sieve_range(lo, b, out, cursor, deep, st, large->bits, shape);
         if (rc) return rc;
         a = b;
     }
@@ -491,6 +491,7 @@ struct ww_ctx {
                               // [3] ww_wallsunsun, [4] ww_count_prps, [5 + i] host chunk i
     // the large deep primes of ww_sieve_prp / ww_count_prps (ww_set_sieve_depth)
     int sieve_depth = kDefaultSieveDepth;
+    int sieve_shape = 0;  // ww_set_sieve_shape
     LargeMarks large{{nullptr, 0}, nullptr, 0};
 };
 
@@ -679,7 +680,20 @@ int ww_sieve_prp(ww_ctx *c, uint64_t kernel_start, uint64_t stop, int32_t wheel_
     const int rc = context_large_marks(c, &large);
     if (rc) return rc;
     return launch_sieve(kernel_start, stop, wheel_idx, (uint64_t *)c->prime, (uint64_t *)c->inv, c->dc->primecount,
-                        c->cap, &c->dc->overflow, c->stream, c->d_cursor + 1, large);
+                        c->cap, &c->dc->overflow, c->stream, c->d_cursor + 1, large, c->sieve_shape);
+}
+
+int ww_set_sieve_shape(ww_ctx *c, int shape) {
+    if (!c) return set_err("null context"), WW_ERR_ARG;
+    if (shape < 0 || shape > 2) return set_err("sieve shape %d: 0 (by width), 1 (wide) or 2 (narrow)", shape), WW_ERR_ARG;
+    c->sieve_shape = shape;
+    return WW_OK;
+}
+
+int ww_get_sieve_shape(ww_ctx *c, int *shape) {
+    if (!c || !shape) return set_err("null argument"), WW_ERR_ARG;
+    *shape = c->sieve_shape;
+    return WW_OK;
 }
 
 int ww_set_sieve_depth(ww_ctx *c, int bits) {
@@ -827,7 +841,7 @@ int ww_count_prps(ww_ctx *c, uint64_t lo, uint64_t hi, uint64_t *count) {
             int rc = context_large_marks(c, &large);
             if (rc) return rc;
             rc = launch_sieve(ks, b, idx, nullptr, nullptr, c->d_count, 0, c->d_count + 2, c->stream,
-                              c->d_cursor + 4, large);
+                              c->d_cursor + 4, large, c->sieve_shape);
             if (rc) return rc;
             u32 n = 0;
             WW_CU(cudaMemcpyAsync(&n, c->d_count, sizeof(u32), cudaMemcpyDeviceToHost, c->stream));

@@ -326,8 +326,41 @@ uint64_t autotune(ww_ctx *ctx, uint64_t current, uint64_t top, double target_ms,
         width = (uint64_t)std::min(nw, (double)kMaxRange);
         if (stop == top) break;
     }
-    fprintf(stderr, "Kernel profile: %0.3f ms. Worksize: %" PRIu64 "\n", ms, width);
-    if (debug) printf("Kernel profile: %0.3f ms. Worksize: %" PRIu64 "\n", ms, width);
+    // then the sieve's segment shape and depth: one segment of the chosen
+    // width timed for each, the fastest kept in the context (results do not
+    // depend on either)
+    uint64_t stop = start + std::min<uint64_t>(width, top - start);
+    if (stop < start) stop = top;
+    const int shapes[2] = {1, 2}, depths[4] = {20, 24, 26, 28};
+    int best_shape = 0, best_depth = 20;
+    float best = 0;
+    for (int sh : shapes) {
+        for (int d : depths) {
+            must(ww_set_sieve_shape(ctx, sh), "sieve shape");
+            must(ww_set_sieve_depth(ctx, d), "sieve depth");
+            must(ww_clear_results(ctx), "clearresult");
+            enqueue_segment(ctx, start, stop, separate);  // warm (and builds the depth's table)
+            must(ww_marker(ctx, 5), "marker");
+            enqueue_segment(ctx, start, stop, separate);
+            must(ww_marker(ctx, 6), "marker");
+            must(ww_sync(ctx, 600000), "sync");
+            float m = 0;
+            must(ww_marker_elapsed(ctx, 5, 6, &m), "elapsed");
+            if (best == 0 || m < best) {
+                best = m;
+                best_shape = sh;
+                best_depth = d;
+            }
+        }
+    }
+    must(ww_set_sieve_shape(ctx, best_shape), "sieve shape");
+    must(ww_set_sieve_depth(ctx, best_depth), "sieve depth");
+    must(ww_clear_results(ctx), "clearresult");
+    fprintf(stderr, "Kernel profile: %0.3f ms. Worksize: %" PRIu64 ". Sieve shape %d, depth %d: %0.3f ms\n", ms, width,
+            best_shape, best_depth, best);
+    if (debug)
+        printf("Kernel profile: %0.3f ms. Worksize: %" PRIu64 ". Sieve shape %d, depth %d: %0.3f ms\n", ms, width,
+               best_shape, best_depth, best);
     return std::max<uint64_t>(width, 1ull << 20);
 }
 

@@ -111,6 +111,8 @@ _SIGS = {
     "ww_sieve_prp": (C.c_int, [_VP, C.c_uint64, C.c_uint64, C.c_int32]),
     "ww_set_sieve_depth": (C.c_int, [_VP, C.c_int]),
     "ww_get_sieve_depth": (C.c_int, [_VP, C.POINTER(C.c_int)]),
+    "ww_set_sieve_shape": (C.c_int, [_VP, C.c_int]),
+    "ww_get_sieve_shape": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "ww_wieferich": (C.c_int, [_VP]),
     "ww_wallsunsun": (C.c_int, [_VP]),
     "ww_test_prps": (C.c_int, [_VP]),
@@ -338,6 +340,15 @@ class Context:
         b = C.c_int(0)
         check(_L.ww_get_sieve_depth(self.h, C.byref(b)), "ww_get_sieve_depth")
         return b.value
+
+    def set_sieve_shape(self, shape: int) -> None:
+        """Sieve segments: 1 wide (2^20 numbers, 512 threads), 2 narrow (2^19, 256), 0 by width."""
+        check(_L.ww_set_sieve_shape(self.h, shape), "ww_set_sieve_shape")
+
+    def sieve_shape(self) -> int:
+        v = C.c_int(0)
+        check(_L.ww_get_sieve_shape(self.h, C.byref(v)), "ww_get_sieve_shape")
+        return v.value
 
     def wieferich(self):
         check(_L.ww_wieferich(self.h), "ww_wieferich")
