@@ -435,6 +435,20 @@ WW_HD D2 m2_small(u64 L, D2 one, u64 p, double rp) {
     return r;
 }
 
+// X 2^v mod p^2 for v < 16 (a plain multiple, so Montgomery form is kept):
+// x0 2^v = d0 + p q0, then d1 = (x1 2^v + q0) mod p, both below 2^16 p.
+WW_HD D2 m2_mul_pow2(D2 x, u32 v, u64 p, double rp) {
+    u64 q0, q1;
+    D2 r;
+    const u64 h0 = v ? x.d0 >> (64 - v) : 0;
+    r.d0 = mod_est(h0, x.d0 << v, p, rp, q0);
+    u64 h1 = v ? x.d1 >> (64 - v) : 0;
+    const u64 l1 = (x.d1 << v) + q0;
+    h1 += (u64)(l1 < q0);
+    r.d1 = mod_est(h1, l1, p, rp, q1);
+    return r;
+}
+
 // x / 5 mod p for 0 <= x < p, p prime to 5; also returns j with 5y = x + j p.
 WW_HD u64 div5_mod(u64 x, u64 p, u32 pm5, u32 &j) {
     // inverse of p mod 5 for residues 1..4: 1, 3, 2, 4

@@ -113,6 +113,7 @@ struct LadderStart {
     int i0, iw;
     bool odd;  // parity of the Lucas index k0
     D2 a, b, w;
+    double rp;  // 1 / (double)p
 };
 
 WW_HD LadderStart ladder_start(u64 p, u64 n, D2 one) {
@@ -123,6 +124,7 @@ WW_HD LadderStart ladder_start(u64 p, u64 n, D2 one) {
     const u32 k0 = (u32)(n >> (st.i0 + 1));
     const u32 e0 = (u32)(e >> (st.iw + 1));
     const double rp = 1.0 / (double)p;
+    st.rp = rp;
     st.odd = k0 & 1u;
     st.a = m2_small(lucas_small(k0), one, p, rp);
     st.b = m2_small(lucas_small(k0 + 1), one, p, rp);
@@ -209,7 +211,12 @@ WW_HD void both_digits_t(u64 p, u64 q, D2 one, D2 &s_out, D2 &c_out) {
         const D2 b2 = ar.sqr(b);
         if (i <= st.iw) {
             w = ar.sqr(w);
+#if defined(WW_W_WINDOW)
+            // every fourth bit from iw down: w *= 2^v for the group's four bits
+            if (((st.iw - i) & 3) == 3) w = m2_mul_pow2(w, (u32)(e >> i) & 15u, p, st.rp);
+#else
             w = sel((e >> i) & 1, m2_dbl(w, p), w);
+#endif
         }
         const D2 c = sel(odd, two, mtwo);     // -2(-1)^k
         const D2 v2k = m2_add(a2, c, p);      // V_2k
@@ -219,6 +226,10 @@ WW_HD void both_digits_t(u64 p, u64 q, D2 one, D2 &s_out, D2 &c_out) {
         b = sel(bit, v2k2, v2k1);
         odd = bit;
     }
+#if defined(WW_W_WINDOW)
+    const int rest = (st.iw + 1) & 3;  // the last, partial group of bits
+    if (rest) w = m2_mul_pow2(w, (u32)e & ((1u << rest) - 1u), p, st.rp);
+#endif
     s_out = ar.redc(w);
     c_out = m2_div5(ar.redc(m2_sub(m2_dbl(b, p), a, p)), p);
 }
