@@ -140,11 +140,20 @@ WW_HD D2 wieferich_digits_t(u64 p, u64 q, D2 one) {
     const A ar(p, q);
     const u64 e = p >> 1;
     const int i0 = top_bit(e) - 5;
-    D2 a = m2_small(1ull << (u32)(e >> (i0 + 1)), one, p, 1.0 / (double)p);
+    const double rp = 1.0 / (double)p;
+    D2 a = m2_small(1ull << (u32)(e >> (i0 + 1)), one, p, rp);
     for (int i = i0; i >= 0; --i) {
         a = ar.sqr(a);
+#if defined(WW_W_WINDOW)
+        if (((i0 - i) & 3) == 3) a = m2_mul_pow2(a, (u32)(e >> i) & 15u, p, rp);
+#else
         a = sel((e >> i) & 1, m2_dbl(a, p), a);
+#endif
     }
+#if defined(WW_W_WINDOW)
+    const int rest = (i0 + 1) & 3;
+    if (rest) a = m2_mul_pow2(a, (u32)e & ((1u << rest) - 1u), p, rp);
+#endif
     return ar.redc(a);
 }
 
