@@ -66,6 +66,8 @@ def test_separate_kernels_and_ckpt_cadence(tests_txt, tmp_path):
     lines = (tmp_path / "results-WWocl.txt").read_text().splitlines()
     assert lines == c["hits"] + [c["checksum"]]
     assert r.stdout.count("Checkpoint, current:") == 30  # 6e10 numbers / 2e9
+    # the autotune picked a sieve shape and depth on the device (in place of profileGPU)
+    assert "Sieve shape" in r.stderr and "depth" in r.stderr
 
 
 def test_resume_from_checkpoint(tests_txt, tmp_path):
