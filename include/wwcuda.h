@@ -165,6 +165,12 @@ int ww_sieve_prp(ww_ctx *ctx, uint64_t kernel_start, uint64_t stop, int32_t whee
  * ww_launch_getsegprimes, which gets no scratch, always sieves at depth 20. */
 int ww_set_sieve_depth(ww_ctx *ctx, int bits);
 int ww_get_sieve_depth(ww_ctx *ctx, int *bits);
+/* Rows first .. first+n-1 of the device's prime table of that depth (the
+ * primes 2^20 < r < 2^bits in ascending order, with ord_r(2)) and its
+ * length in *total, for checking the table against an independent
+ * computation.  Builds the table when it does not exist yet. */
+int ww_selftest_deep_table(ww_ctx *ctx, int bits, uint64_t first, uint64_t n, uint32_t *r, uint32_t *order,
+                           uint64_t *total);
 
 /* Segment shape of the context's sieve launches (no reference counterpart;
  * with the depth, what the program's autotune picks in place of the

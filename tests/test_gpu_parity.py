@@ -104,6 +104,45 @@ def test_sieve_shapes_give_the_same_prp_set(ww, ref_prps):
             c.set_sieve_shape(3)
 
 
+def _order_of_two(r: int) -> int:
+    m, fac, d = r - 1, [], 2
+    x = m
+    while d * d <= x:
+        if x % d == 0:
+            fac.append(d)
+            while x % d == 0:
+                x //= d
+        d += 1
+    if x > 1:
+        fac.append(x)
+    o = m
+    for q in fac:
+        while o % q == 0 and pow(2, o // q, r) == 1:
+            o //= q
+    return o
+
+
+def test_large_prime_table_orders(ww):
+    """The device's table of large deep primes (built by a sieve on the host
+    and an order kernel) against an independent computation: the first and
+    last 1500 rows at depth 26 are the primes there, with ord_r(2) exact --
+    an order too large would let the sieve mark a pseudoprime -- and the
+    table's length is the prime count of (2^20, 2^26)."""
+    import itertools
+
+    import sympy
+
+    with ww.Context(0, max_prps=1 << 10, max_hits=1024) as c:
+        r0, o0, total = c.deep_table(26, 0, 1500)
+        assert total == sympy.primepi(2**26) - sympy.primepi(2**20)
+        r1, o1, _ = c.deep_table(26, total - 1500, 1500)
+    want0 = [int(p) for p in itertools.islice(sympy.primerange(2**20, 2**26), 1500)]
+    assert [int(x) for x in r0] == want0
+    assert [int(x) for x in r1] == [int(p) for p in sympy.primerange(2**26 - 60000, 2**26)][-1500:]
+    for r, o in list(zip(r0, o0)) + list(zip(r1, o1)):
+        assert int(o) == _order_of_two(int(r)), r
+
+
 def test_count_prps_depths_agree_to_2p32(ww):
     """[127, 2^32) holds every deep prime and many base-2 pseudoprimes with a
     factor above 2^20: its PRP count is the same at depths 20 and 30."""

@@ -182,6 +182,26 @@ int deep_large_device(int bits, DeepLarge *out) {
     return WW_OK;
 }
 
+int read_deep_large(int bits, uint64_t first, uint64_t n, uint32_t *r, uint32_t *o, uint64_t *total) {
+    DeepLarge t{nullptr, 0};
+    const int rc = deep_large_device(bits, &t);
+    if (rc) return rc;
+    *total = t.n;
+    if (first >= t.n) return WW_OK;
+    if (n > t.n - first) n = t.n - first;
+    std::vector<DeepRow> rows(n);
+    const cudaError_t e = cudaMemcpy(rows.data(), t.rows + first, n * sizeof(DeepRow), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        set_err("deep-sieve table read: %s", cudaGetErrorString(e));
+        return WW_ERR_CUDA;
+    }
+    for (uint64_t i = 0; i < n; ++i) {
+        r[i] = rows[i].r;
+        o[i] = rows[i].o;
+    }
+    return WW_OK;
+}
+
 int launch_deep_fill(u64 first, u64 nodd, const DeepLarge &t, u32 *bits, u64 nwords, cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(bits, 0, nwords * sizeof(u32), stream);
     if (e == cudaSuccess && t.n) {

@@ -22,6 +22,10 @@ struct DeepLarge {
 // sieve and one kernel; cached until the process exits).
 int deep_large_device(int bits, DeepLarge *out);
 
+// Rows first .. first+n-1 of the table of `bits` on the current device
+// (r and ord_r(2)), and the table's length, for checking the table.
+int read_deep_large(int bits, uint64_t first, uint64_t n, uint32_t *r, uint32_t *o, uint64_t *total);
+
 // Zero bits[0, nwords) and mark, for the odd numbers first + 2j (j < nodd),
 // the multiples of the table's primes that the cofactor rule marks.
 int launch_deep_fill(u64 first, u64 nodd, const DeepLarge &t, u32 *bits, u64 nwords, cudaStream_t stream);

@@ -715,6 +715,13 @@ int ww_set_sieve_depth(ww_ctx *c, int bits) {
     return WW_OK;
 }
 
+int ww_selftest_deep_table(ww_ctx *c, int bits, uint64_t first, uint64_t n, uint32_t *r, uint32_t *order,
+                           uint64_t *total) {
+    if (!c || !total || ((!r || !order) && n)) return set_err("null argument"), WW_ERR_ARG;
+    WW_CU(cudaSetDevice(c->device));
+    return read_deep_large(bits, first, n, r, order, total);
+}
+
 int ww_get_sieve_depth(ww_ctx *c, int *bits) {
     if (!c || !bits) return set_err("null argument"), WW_ERR_ARG;
     *bits = c->sieve_depth;

@@ -111,6 +111,8 @@ _SIGS = {
     "ww_sieve_prp": (C.c_int, [_VP, C.c_uint64, C.c_uint64, C.c_int32]),
     "ww_set_sieve_depth": (C.c_int, [_VP, C.c_int]),
     "ww_get_sieve_depth": (C.c_int, [_VP, C.POINTER(C.c_int)]),
+    "ww_selftest_deep_table": (C.c_int, [_VP, C.c_int, C.c_uint64, C.c_uint64, _VP, _VP,
+                                         C.POINTER(C.c_uint64)]),
     "ww_set_sieve_shape": (C.c_int, [_VP, C.c_int]),
     "ww_get_sieve_shape": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "ww_wieferich": (C.c_int, [_VP]),
@@ -340,6 +342,16 @@ class Context:
         b = C.c_int(0)
         check(_L.ww_get_sieve_depth(self.h, C.byref(b)), "ww_get_sieve_depth")
         return b.value
+
+    def deep_table(self, bits: int, first: int, n: int) -> tuple[np.ndarray, np.ndarray, int]:
+        """Rows of the device's large-prime table: (r, ord_r(2), table length)."""
+        r = np.zeros(max(n, 1), np.uint32)
+        o = np.zeros(max(n, 1), np.uint32)
+        tot = C.c_uint64(0)
+        check(_L.ww_selftest_deep_table(self.h, bits, first, n, r.ctypes.data, o.ctypes.data, C.byref(tot)),
+              "ww_selftest_deep_table")
+        m = max(0, min(n, tot.value - first))
+        return r[:m], o[:m], tot.value
 
     def set_sieve_shape(self, shape: int) -> None:
         """Sieve segments: 1 wide (2^20 numbers, 512 threads), 2 narrow (2^19, 256), 0 by width."""
