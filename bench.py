@@ -278,6 +278,16 @@ def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30, chain_pe
             "executed_ops_per_prime": run_ops, "frac_executed_ops": rate * run_ops / chain_peak,
             "note": "reference ops count the reference algorithm's work (more SPRP candidates, a longer "
                     "Lucas ladder); above 1.0 means less work than the reference needs, not above peak"}
+        # the sieve kernel alone over one 2^30-number segment: its multiplies
+        # are the SPRP tests of the candidates it leaves (estimated from the
+        # depth as above; the sieving itself is shifts, ORs and atomics)
+        seg = out["segment_2p30"]
+        cand_per_number = cand / np.log(2.0**64)
+        sieve_ops = cand_per_number * (20.0 * (k - 5) + 12.0) * min(width, ckpt)
+        out["sieve_roofline"] = {"executed_ops_per_number": cand_per_number * (20.0 * (k - 5) + 12.0),
+                                 "achieved_tops": sieve_ops / (seg["sieve_ms"] * 1e-3) / 1e12,
+                                 "frac_chain_peak": sieve_ops / (seg["sieve_ms"] * 1e-3) / chain_peak,
+                                 "note": "candidates per number estimated as 0.5615 / ln 2^depth (Mertens)"}
     golden = ROOT / "tests" / "golden" / "ref_long.json"
     if golden.exists():
         g = json.loads(golden.read_text())["config3"]
@@ -496,6 +506,7 @@ def summarize(line: dict, extra: dict) -> dict:
         out["config3_plain_range"] = {"primes_per_s": r(g["primes_per_s"], 4), "numbers_per_s": r(g["numbers_per_s"], 4),
                                       "sieve_ms_2p30": r(g["segment_2p30"]["sieve_ms"]),
                                       "test_ms_2p30": r(g["segment_2p30"]["test_ms"]),
+                                      "sieve_frac_chain_peak": r((g.get("sieve_roofline") or {}).get("frac_chain_peak")),
                                       "checksum": g["checksum"],
                                       "checksum_equal_reference": g.get("reference_checksum_equal")}
     if "batched_vs_plain" in extra:
