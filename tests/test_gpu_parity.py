@@ -143,6 +143,35 @@ def test_large_prime_table_orders(ww):
         assert int(o) == _order_of_two(int(r)), r
 
 
+@pytest.mark.parametrize("tail", [12345, (1 << 19) + 777, (1 << 20) - 3])
+def test_split_last_round_equals_single_round_pieces(ww, tail):
+    """A launch of 396 whole 2^20-number segments plus a partial one (more
+    than the 296 resident CTAs, a last round short enough to be split into
+    half segments, whose last half may lie past the range's end) gives the
+    same PRP list as the range sieved in pieces of one round each."""
+    lo = 2**63 + 2**40 + 1
+    hi = lo + (396 << 20) + tail
+    with ww.Context(0, max_prps=ww.prp_count_bound(lo, hi), max_hits=15000) as c:
+        c.set_sieve_shape(1)
+        c.clear_results()
+        c.clear_segment()
+        c.sieve_prp(lo, hi)
+        c.sync()
+        whole = _digest(c.prps())
+        n_whole = c.count_prps(lo, hi)
+        parts = []
+        a = lo
+        while a < hi:
+            b = min(a + (200 << 20), hi)
+            c.clear_segment()
+            c.sieve_prp(a, b)
+            c.sync()
+            parts.append(c.prps())
+            a = b
+    assert whole == _digest(np.concatenate(parts))
+    assert n_whole == whole[0]
+
+
 def test_count_prps_depths_agree_to_2p32(ww):
     """[127, 2^32) holds every deep prime and many base-2 pseudoprimes with a
     factor above 2^20: its PRP count is the same at depths 20 and 30."""

@@ -60,7 +60,8 @@ __global__ void __launch_bounds__(G::kThreads, 1024 / G::kThreads) k_sieve_prp(u
                                      : nfull * (u64)G::kOdd + (item - nfull) * (u64)(G::kOdd / 2);
         const u64 len = item < nfull ? (u64)G::kOdd : (u64)(G::kOdd / 2);
         const u64 seg_off = 2 * off;
-        const u64 rem_span = span - seg_off;  // > 0
+        // the second half of a partial last segment may start past the end
+        const u64 rem_span = seg_off < span ? span - seg_off : 0;
         const u64 nvalid = (rem_span / 2 < len) ? rem_span / 2 : len;
 
         // ---- pre-sieve 3..113 on this thread's contiguous words
