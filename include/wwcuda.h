@@ -161,7 +161,7 @@ int ww_sieve_prp(ww_ctx *ctx, uint64_t kernel_start, uint64_t stop, int32_t whee
  * per launch (bits <= 30; the first use of a depth on a device builds its
  * prime table).  Only composites that can never be base-2 pseudoprimes are
  * marked, so the PRP list is the same at every depth.  A new context sieves
- * at depth 26; depth 20 turns the large primes off.  The kernel-shaped
+ * at depth 28; depth 20 turns the large primes off.  The kernel-shaped
  * ww_launch_getsegprimes, which gets no scratch, always sieves at depth 20. */
 int ww_set_sieve_depth(ww_ctx *ctx, int bits);
 int ww_get_sieve_depth(ww_ctx *ctx, int *bits);

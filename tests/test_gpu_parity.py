@@ -144,11 +144,11 @@ def test_large_prime_table_orders(ww):
 
 
 @pytest.mark.parametrize("tail", [12345, (1 << 19) + 777, (1 << 20) - 3])
-def test_split_last_round_equals_single_round_pieces(ww, tail):
-    """A launch of 396 whole 2^20-number segments plus a partial one (more
-    than the 296 resident CTAs, a last round short enough to be split into
-    half segments, whose last half may lie past the range's end) gives the
-    same PRP list as the range sieved in pieces of one round each."""
+def test_multi_round_launch_equals_single_round_pieces(ww, tail):
+    """A launch of 396 whole 2^20-number segments plus a partial one of
+    several lengths (more segments than the 296 resident CTAs take in one
+    round, with the large deep primes' marks) gives the same PRP list as the
+    range sieved in pieces of one round each."""
     lo = 2**63 + 2**40 + 1
     hi = lo + (396 << 20) + tail
     with ww.Context(0, max_prps=ww.prp_count_bound(lo, hi), max_hits=15000) as c:

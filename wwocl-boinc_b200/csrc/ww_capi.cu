@@ -292,18 +292,8 @@ int launch_sieve_shape(uint64_t low, uint64_t high, uint64_t span, const PrpOut 
     int slots = 0;
     WW_CU(sieve_slots<G>(&slots));
     const uint64_t grid = nseg < (uint64_t)slots ? nseg : (uint64_t)slots;
-    // a last round of at most half the resident CTAs is taken in half
-    // segments: it then ends about half a segment's time after the others
-    // instead of a whole one (2^30 numbers: 1024 wide segments for 296 CTAs,
-    // 3.5 rounds instead of 4)
-    uint64_t nfull = nseg;
-    if (nseg > grid) {
-        const uint64_t r = nseg % grid;
-        if (r && r <= grid / 2) nfull = nseg - r;
-    }
     if (cursor) WW_CU(cudaMemsetAsync(cursor, 0, sizeof(u64), stream));
-    k_sieve_prp<G><<<(unsigned)grid, G::kThreads, G::kSmem, stream>>>(low, high, nseg, nfull, out, cursor, deep,
-                                                                         marks);
+    k_sieve_prp<G><<<(unsigned)grid, G::kThreads, G::kSmem, stream>>>(low, high, nseg, out, cursor, deep, marks);
     WW_CHECK_LAUNCH();
     return WW_OK;
 }
@@ -475,7 +465,7 @@ void destroy_server_state(ServerState *s);
 // Sieve depth of a new context: the deep primes below 2^kDefaultSieveDepth
 // (ww_set_sieve_depth).
 #ifndef WW_SIEVE_DEPTH
-#define WW_SIEVE_DEPTH 26
+#define WW_SIEVE_DEPTH 28
 #endif
 constexpr int kDefaultSieveDepth = WW_SIEVE_DEPTH;
 

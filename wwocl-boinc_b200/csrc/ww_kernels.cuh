@@ -27,15 +27,12 @@ namespace ww {
 // With a segment cursor (zeroed before the launch) the CTAs take segments
 // one at a time from it; without one (a launch captured into a graph, or
 // one that found every cursor of the library's pool busy) they stride over
-// the segments.  The segments from nfull on are taken in halves (work
-// item nfull + 2h + k is half k of segment nfull + h), so that a short last
-// round of segments ends about as early on every SM.  marks (optional): the
-// large deep primes' marks of the whole launch, bit j of word w = odd number
-// b0 + 2(32 w + j) + 1 (ww_bucket.cu), ORed into each segment's bitmap.
+// the segments.  marks (optional): the large deep primes' marks of the whole
+// launch, bit j of word w = odd number b0 + 2(32 w + j) + 1 (ww_bucket.cu),
+// ORed into each segment's bitmap.
 template <class G>
-__global__ void __launch_bounds__(G::kThreads, 1024 / G::kThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, u64 nfull,
-                                                                              PrpOut out, u64 *cursor,
-                                                                              const DeepRow *deep,
+__global__ void __launch_bounds__(G::kThreads, 1024 / G::kThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out,
+                                                                              u64 *cursor, const DeepRow *deep,
                                                                               const u32 *__restrict__ marks) {
     extern __shared__ u32 sieve_smem[];  // G::kSmem bytes
     u32 *bitmap = sieve_smem;
@@ -47,30 +44,22 @@ __global__ void __launch_bounds__(G::kThreads, 1024 / G::kThreads) k_sieve_prp(u
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
 
-    const u64 nitems = nfull + 2 * (nseg - nfull);
-    u64 item = blockIdx.x;
+    u64 seg = blockIdx.x;
     if (cursor) {
         if (threadIdx.x == 0) s_seg = atomicAdd((unsigned long long *)cursor, 1ull);
         __syncthreads();
-        item = s_seg;
+        seg = s_seg;
     }
-    while (item < nitems) {
-        // odd-number offset and length of the work item
-        const u64 off = item < nfull ? item * (u64)G::kOdd
-                                     : nfull * (u64)G::kOdd + (item - nfull) * (u64)(G::kOdd / 2);
-        const u64 len = item < nfull ? (u64)G::kOdd : (u64)(G::kOdd / 2);
-        const u64 seg_off = 2 * off;
-        // the second half of a partial last segment may start past the end
-        const u64 rem_span = seg_off < span ? span - seg_off : 0;
-        const u64 nvalid = (rem_span / 2 < len) ? rem_span / 2 : len;
+    while (seg < nseg) {
+        const u64 seg_off = seg * (u64)(2 * G::kOdd);
+        const u64 rem_span = span - seg_off;  // > 0
+        const u64 nvalid = (rem_span / 2 < (u64)G::kOdd) ? rem_span / 2 : (u64)G::kOdd;
 
         // ---- pre-sieve 3..113 on this thread's contiguous words
-        const int w0 = threadIdx.x * G::kWordsPerThread;
-        if ((u64)w0 * 32 >= nvalid) {  // all past the item's end
-            for (int w = w0; w < w0 + G::kWordsPerThread; ++w) bitmap[w] = ~0u;
-        } else {
+        {
+            const int w0 = threadIdx.x * G::kWordsPerThread;
             const u64 n0 = b0 + seg_off + 64ull * (u64)w0 + 1;  // may wrap past 2^64 beyond hi
-            const u32 *seg_marks = marks ? marks + off / 32 : nullptr;
+            const u32 *seg_marks = marks ? marks + seg * (u64)G::kWords : nullptr;
 #define WW_J0(R) u32 j##R = first_hit<R>(n0);
             WW_FOR_SMALL_PRIMES(WW_J0)
 #undef WW_J0
@@ -102,12 +91,11 @@ __global__ void __launch_bounds__(G::kThreads, 1024 / G::kThreads) k_sieve_prp(u
         // warp queue and PRP-test them 32 at a time
         u32 *q = queue[warp];
         int qn = 0;
-        const u32 nchunks = (u32)((nvalid + 1023) / 1024);  // 32-word chunks holding valid bits
         for (;;) {
             u32 chunk = 0;
             if (lane == 0) chunk = atomicAdd(&s_chunk, 1u);
             chunk = __shfl_sync(0xffffffffu, chunk, 0);
-            const bool more = chunk < nchunks;
+            const bool more = chunk < (u32)(G::kWords / 32);
             if (more) {
                 const int w = chunk * 32 + lane;
                 u32 cand = ~bitmap[w];
@@ -138,13 +126,13 @@ __global__ void __launch_bounds__(G::kThreads, 1024 / G::kThreads) k_sieve_prp(u
             }
             if (!more) break;
         }
-        __syncthreads();  // bitmap reused by the next work item
+        __syncthreads();  // bitmap reused by the next segment
         if (cursor) {
             if (threadIdx.x == 0) s_seg = atomicAdd((unsigned long long *)cursor, 1ull);
             __syncthreads();
-            item = s_seg;
+            seg = s_seg;
         } else {
-            item += gridDim.x;
+            seg += gridDim.x;
         }
     }
 }
