@@ -159,7 +159,10 @@ int ww_sieve_prp(ww_ctx *ctx, uint64_t kernel_start, uint64_t stop, int32_t whee
  * below 2^20 segment by segment; at depth bits > 20, a launch of 2^26
  * numbers or more also marks the multiples of the primes below 2^bits, once
  * per launch (bits <= 30; the first use of a depth on a device builds its
- * prime table).  Only composites that can never be base-2 pseudoprimes are
+ * prime table, which allocates device memory and synchronises the device,
+ * so it belongs before any stream capture; each context also allocates a
+ * 64 MiB mark bitmap on its first such launch).  Only composites that can
+ * never be base-2 pseudoprimes are
  * marked, so the PRP list is the same at every depth.  A new context sieves
  * at depth 28; depth 20 turns the large primes off.  The kernel-shaped
  * ww_launch_getsegprimes, which gets no scratch, always sieves at depth 20. */
