@@ -162,10 +162,10 @@ int ww_sieve_prp(ww_ctx *ctx, uint64_t kernel_start, uint64_t stop, int32_t whee
  * prime table, which allocates device memory and synchronises the device,
  * so it belongs before any stream capture; each context also allocates a
  * 64 MiB mark bitmap on its first such launch).  Only composites that can
- * never be base-2 pseudoprimes are
- * marked, so the PRP list is the same at every depth.  A new context sieves
- * at depth 28; depth 20 turns the large primes off.  The kernel-shaped
- * ww_launch_getsegprimes, which gets no scratch, always sieves at depth 20. */
+ * never be base-2 pseudoprimes are marked, so the PRP list is the same at
+ * every depth.  A new context sieves at depth 28; depth 20 turns the large
+ * primes off.  The kernel-shaped ww_launch_getsegprimes, which gets no
+ * scratch, always sieves at depth 20. */
 int ww_set_sieve_depth(ww_ctx *ctx, int bits);
 int ww_get_sieve_depth(ww_ctx *ctx, int *bits);
 /* Rows first .. first+n-1 of the device's prime table of that depth (the
