@@ -141,6 +141,11 @@ def test_large_prime_table_orders(ww):
     assert [int(x) for x in r1] == [int(p) for p in sympy.primerange(2**26 - 60000, 2**26)][-1500:]
     for r, o in list(zip(r0, o0)) + list(zip(r1, o1)):
         assert int(o) == _order_of_two(int(r)), r
+    # a large prime of small order: 616318177 divides 2^37 - 1 (depth 30)
+    idx = int(sympy.primepi(616318177) - sympy.primepi(2**20)) - 1
+    with ww.Context(0, max_prps=1 << 10, max_hits=1024) as c:
+        r2, o2, _ = c.deep_table(30, idx, 1)
+    assert (int(r2[0]), int(o2[0])) == (616318177, 37)
 
 
 @pytest.mark.parametrize("tail", [12345, (1 << 19) + 777, (1 << 20) - 3])

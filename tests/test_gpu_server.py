@@ -159,21 +159,22 @@ def test_calls_out_of_order_are_refused(ww, ctx):
 
 def test_requests_admitted_mid_flight_equal_alone_and_oracle(ww, ctx, oracle):
     """Continuous batching: requests are submitted between steps while
-    others are on the device (widths across two decades, 1e5 to 1e7, plus
-    the known Wieferich and WSS windows).  Every finished request equals its
+    others are on the device (widths across two decades, 2e5 to 2e7, plus
+    the known Wieferich and WSS windows; two tiles of 2^20 numbers per step,
+    so most requests take several steps).  Every finished request equals its
     run alone through the context API and the oracle: checksum, PRP count,
     hit records and PRP list."""
-    units = ww.uneven_units(29, 30, wmin=1e5, wmax=1e7, smin=10**12, smax=2**64 - 10**8)
+    units = ww.uneven_units(29, 30, wmin=2e5, wmax=2e7, smin=10**12, smax=2**64 - 10**8)
     reqs = [(5000 + i, a, b) for i, (a, b) in enumerate(units)]
     reqs.insert(7, (4998, 2276306935816523 - 5000, 2276306935816523 + 5000))
     reqs.insert(15, (4999, 338772621946054253 - 5000, 338772621946054253 + 5000))
-    srv = ww.Server(ctx, prp_pool_bytes=1 << 28, max_active=8, epoch_tiles=12, store_prps=True)
+    srv = ww.Server(ctx, prp_pool_bytes=1 << 28, max_active=8, epoch_tiles=2, store_prps=True)
     pending = list(reqs)
     srv.submit(pending[:5])
     pending = pending[5:]
     got, admitted_while_busy, steps = {}, 0, 0
     while len(got) < len(reqs) and steps < 20000:
-        if pending and steps % 2 == 1:  # two more requests every other step
+        if pending and steps % 2 == 1:  # two more requests every other step, while others run
             q, active, _ = srv.status()
             admitted_while_busy += active > 0
             srv.submit(pending[:2])

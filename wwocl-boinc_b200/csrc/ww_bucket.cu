@@ -79,8 +79,8 @@ __device__ u32 pow2_mod(u32 e, u32 r) {  // 2^e mod r for e >= 1, r < 2^30
 
 // One table row per prime: o = ord_r(2) from the prime factors of r - 1
 // (trial division by the odd primes below 2^15; r - 1 < 2^30 has at most
-// nine distinct prime factors), and the constants of deep_start.
-__global__ void k_deep_orders(const u32 *primes, u32 n, const u32 *small, u32 nsmall, DeepRow *rows) {
+// nine distinct prime factors).
+__global__ void k_deep_orders(const u32 *primes, u32 n, const u32 *small, u32 nsmall, DeepPrime *rows) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const u32 r = primes[i];
@@ -101,21 +101,33 @@ __global__ void k_deep_orders(const u32 *primes, u32 n, const u32 *small, u32 ns
     u32 o = r - 1;
     for (int f = 0; f < nf; ++f)
         while (o % fac[f] == 0 && pow2_mod(o / fac[f], r) == 1) o /= fac[f];
-    DeepRow e;
-    e.r = r;
-    e.o = o;
-    e.rinv = inv64(r);
-    e.mr = ~0ull / r;  // floor(2^64 / r): r is odd and above 1
-    e.mo = (o & (o - 1)) ? ~0ull / o : (1ull << (65 - __ffs((int)o)));  // exact for a power of two
-    rows[i] = e;
+    // floor(2^64 / o), exact (a power of two divides 2^64)
+    rows[i] = DeepPrime{r, o, (o & (o - 1)) ? ~0ull / o : (1ull << (65 - __ffs((int)o)))};
+}
+
+// floor(2^64 / d) for odd 2^11 < d < 2^32: the quotient is below 2^53, so a
+// double-precision estimate is within one of it, and one exact correction
+// finishes.
+__device__ __forceinline__ u64 floor_2p64_div(u64 d) {
+    u64 q = (u64)(18446744073709551616.0 / (double)d);
+    if (mul_hi(q, d) != 0) --q;  // q d > 2^64 - 1
+    if (0 - q * d >= d) ++q;     // 2^64 - q d >= d
+    return q;
 }
 
 // One thread per large prime: its odd multiples first + 2j, j < nodd, that
-// the cofactor rule marks.
-__global__ void k_deep_fill(u64 first, u64 nodd, const DeepRow *__restrict__ rows, u32 n, u32 *bits) {
+// the cofactor rule marks.  The rows are streamed with evict-first loads so
+// that the bitmap the atomics hit stays in L2.
+__global__ void k_deep_fill(u64 first, u64 nodd, const DeepPrime *__restrict__ rows, u32 n, u32 *bits) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const DeepRow e = rows[i];
+    const uint4 row = __ldcs(reinterpret_cast<const uint4 *>(rows) + i);
+    DeepRow e;
+    e.r = row.x;
+    e.o = row.y;
+    e.mo = ((u64)row.w << 32) | row.z;
+    e.rinv = inv64(e.r);
+    e.mr = floor_2p64_div(e.r);
     u32 j0, km;
     deep_start(first, e, j0, km);
     for (u64 j = j0; j < nodd; j += e.r) {
@@ -155,10 +167,10 @@ int deep_large_device(int bits, DeepLarge *out) {
     const std::vector<u32> small = small_odd_primes();
     const std::vector<u32> primes = primes_between((1u << WW_DEEP_BITS) + 1, 1u << bits, small);
     u32 *d_primes = nullptr, *d_small = nullptr;
-    DeepRow *d_rows = nullptr;
+    DeepPrime *d_rows = nullptr;
     cudaError_t e = cudaMalloc(&d_primes, primes.size() * sizeof(u32));
     if (e == cudaSuccess) e = cudaMalloc(&d_small, small.size() * sizeof(u32));
-    if (e == cudaSuccess) e = cudaMalloc(&d_rows, primes.size() * sizeof(DeepRow));
+    if (e == cudaSuccess) e = cudaMalloc(&d_rows, primes.size() * sizeof(DeepPrime));
     if (e == cudaSuccess)
         e = cudaMemcpy(d_primes, primes.data(), primes.size() * sizeof(u32), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d_small, small.data(), small.size() * sizeof(u32), cudaMemcpyHostToDevice);
@@ -189,8 +201,8 @@ int read_deep_large(int bits, uint64_t first, uint64_t n, uint32_t *r, uint32_t 
     *total = t.n;
     if (first >= t.n) return WW_OK;
     if (n > t.n - first) n = t.n - first;
-    std::vector<DeepRow> rows(n);
-    const cudaError_t e = cudaMemcpy(rows.data(), t.rows + first, n * sizeof(DeepRow), cudaMemcpyDeviceToHost);
+    std::vector<DeepPrime> rows(n);
+    const cudaError_t e = cudaMemcpy(rows.data(), t.rows + first, n * sizeof(DeepPrime), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) {
         set_err("deep-sieve table read: %s", cudaGetErrorString(e));
         return WW_ERR_CUDA;

@@ -11,10 +11,21 @@ namespace ww {
 // Deepest table: primes below 2^30 (the rows keep r in 32 bits).
 constexpr int kDeepLargeMaxBits = 30;
 
+// One large deep prime: r, o = ord_r(2) and floor(2^64 / o).  The other
+// constants of its start (r^-1 mod 2^64, floor(2^64 / r)) are recomputed at
+// every launch: 16 bytes a row instead of 32 keep the table's stream from
+// evicting the mark bitmap from L2.  floor(2^64 / o) stays in the row: for
+// small orders (o = 37 for r = 616318177, a factor of 2^37 - 1) the quotient
+// is beyond a double-precision estimate's reach.
+struct __align__(16) DeepPrime {
+    u32 r, o;
+    u64 mo;
+};
+
 // Rows of the primes 2^WW_DEEP_BITS < r < 2^bits on one device, in
 // ascending order.
 struct DeepLarge {
-    const DeepRow *rows;
+    const DeepPrime *rows;
     u32 n;
 };
 
