@@ -12,9 +12,9 @@
 // only when k != 1 (mod ord_r(2)), so every possible base-2 pseudoprime --
 // and r itself -- stays a candidate and the PRP set does not change.
 //
-// The table of large primes (r, ord_r(2) and the start constants) is built
-// once per device and depth: the primes come from a segmented sieve on the
-// host, the orders from a kernel that factors r - 1 by trial division.
+// The table of large primes (r, ord_r(2) and floor(2^64 / ord_r(2))) is
+// built once per device and depth: the primes come from a segmented sieve on
+// the host, the orders from a kernel that factors r - 1 by trial division.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -116,25 +116,29 @@ __device__ __forceinline__ u64 floor_2p64_div(u64 d) {
 }
 
 // Cofactors k of a multiple n = r k that have a factor 3, 5, 7 or 11 (bit
-// k mod 1155 of the CTA's mask): the pre-sieve by 3..113 marks those n in
+// k mod 1155 of a constant mask, copied into each CTA's shared memory): the
+// pre-sieve by 3..113 marks those n in
 // every segment, so the fill skips them -- 58 % of the atomics.
 constexpr u32 kCofWheel = 1155;                       // 3 * 5 * 7 * 11
 constexpr u64 kCofWheelM = 0x38bdba67495d50ull;       // floor(2^64 / 1155)
 constexpr u32 kCofWords = (kCofWheel + 31) / 32;
+struct CofMask {
+    u32 w[kCofWords];
+};
+constexpr CofMask make_cof_mask() {
+    CofMask m{};
+    for (u32 k = 0; k < kCofWheel; ++k)
+        if (k % 3 == 0 || k % 5 == 0 || k % 7 == 0 || k % 11 == 0) m.w[k >> 5] |= 1u << (k & 31);
+    return m;
+}
+__device__ const CofMask g_cof_mask = make_cof_mask();
 
 // One thread per large prime: its odd multiples first + 2j, j < nodd, that
 // the cofactor rule marks.  The rows are streamed with evict-first loads so
 // that the bitmap the atomics hit stays in L2.
 __global__ void k_deep_fill(u64 first, u64 nodd, const DeepPrime *__restrict__ rows, u32 n, u32 *bits) {
     __shared__ u32 s_small[kCofWords];
-    for (u32 w = threadIdx.x; w < kCofWords; w += blockDim.x) {
-        u32 m = 0;
-        for (u32 b = 0; b < 32; ++b) {
-            const u32 k = 32 * w + b;
-            if (k < kCofWheel && (k % 3 == 0 || k % 5 == 0 || k % 7 == 0 || k % 11 == 0)) m |= 1u << b;
-        }
-        s_small[w] = m;
-    }
+    for (u32 w = threadIdx.x; w < kCofWords; w += blockDim.x) s_small[w] = g_cof_mask.w[w];
     __syncthreads();
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
