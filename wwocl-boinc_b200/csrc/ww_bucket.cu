@@ -117,8 +117,8 @@ __device__ __forceinline__ u64 floor_2p64_div(u64 d) {
 
 // Cofactors k of a multiple n = r k that have a factor 3, 5, 7 or 11 (bit
 // k mod 1155 of a constant mask, copied into each CTA's shared memory): the
-// pre-sieve by 3..113 marks those n in
-// every segment, so the fill skips them -- 58 % of the atomics.
+// pre-sieve by 3..113 marks those n in every segment, so the fill skips them
+// -- 58 % of the atomics.
 constexpr u32 kCofWheel = 1155;                       // 3 * 5 * 7 * 11
 constexpr u64 kCofWheelM = 0x38bdba67495d50ull;       // floor(2^64 / 1155)
 constexpr u32 kCofWords = (kCofWheel + 31) / 32;
