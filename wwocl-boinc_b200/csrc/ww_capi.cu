@@ -498,12 +498,13 @@ struct ww_ctx {
 namespace {
 constexpr u64 kHostChunksMax = 1024;
 
-// The context's large deep primes for its sieve launches: nullptr at depth
-// WW_DEEP_BITS; otherwise the table of its depth and the context's mark
-// bitmap (allocated on first use, one piece wide).
-int context_large_marks(ww_ctx *c, LargeMarks **out) {
+// The context's large deep primes for a sieve launch over [lo, hi): nullptr
+// at depth WW_DEEP_BITS or for a launch too narrow to use them; otherwise
+// the table of its depth and the context's mark bitmap (allocated on first
+// use, one piece wide).
+int context_large_marks(ww_ctx *c, u64 lo, u64 hi, LargeMarks **out) {
     *out = nullptr;
-    if (c->sieve_depth <= WW_DEEP_BITS) return WW_OK;
+    if (c->sieve_depth <= WW_DEEP_BITS || hi <= lo || hi - (lo & ~1ull) < kLargeMarksMinSpan) return WW_OK;
     DeepLarge t{nullptr, 0};
     const int rc = deep_large_device(c->sieve_depth, &t);
     if (rc) return rc;
@@ -677,7 +678,7 @@ int ww_sieve_prp(ww_ctx *c, uint64_t kernel_start, uint64_t stop, int32_t wheel_
     ww::TraceRange trace("ww_sieve_prp");
     WW_NEED_BUFFERS(c);
     LargeMarks *large = nullptr;
-    const int rc = context_large_marks(c, &large);
+    const int rc = context_large_marks(c, kernel_start, stop, &large);
     if (rc) return rc;
     return launch_sieve(kernel_start, stop, wheel_idx, (uint64_t *)c->prime, (uint64_t *)c->inv, c->dc->primecount,
                         c->cap, &c->dc->overflow, c->stream, c->d_cursor + 1, large, c->sieve_shape);
@@ -845,7 +846,7 @@ int ww_count_prps(ww_ctx *c, uint64_t lo, uint64_t hi, uint64_t *count) {
         if (ks < b) {
             WW_CU(cudaMemsetAsync(c->d_count, 0, 4 * sizeof(u32), c->stream));
             LargeMarks *large = nullptr;
-            int rc = context_large_marks(c, &large);
+            int rc = context_large_marks(c, ks, b, &large);
             if (rc) return rc;
             rc = launch_sieve(ks, b, idx, nullptr, nullptr, c->d_count, 0, c->d_count + 2, c->stream,
                               c->d_cursor + 4, large, c->sieve_shape);
