@@ -19,7 +19,7 @@
 // different host threads) race on it -- order them on one stream.  The
 // first call on each device does a one-time set-up (the device addresses of
 // the array and of the library's deep-sieve table, and the kernel's
-// shared-memory attribute), which should come before any stream capture.
+// shared-memory attribute).
 #include <cuda_runtime.h>
 
 #include <cstring>
