@@ -324,6 +324,16 @@ def compare_batched_plain(ww, local: int, units: list, workload: str, tune_units
     # WSS kernels with a checkpoint (sync, counters and hits read back,
     # clear) every 2^30 numbers and at the range's end
     ckpt = 1 << 30
+    # warm the plain path as the batched one was: its first launch wide
+    # enough for the large deep primes builds their table and mark bitmap
+    wa = units[0][0]
+    ctx.clear_results()
+    ctx.clear_segment()
+    ctx.sieve_prp(wa, wa + (1 << 27))
+    ctx.wieferich()
+    ctx.wallsunsun()
+    ctx.sync()
+    ctx.clear_results()
     t0 = time.perf_counter()
     plain = []
     for a, z in units:
