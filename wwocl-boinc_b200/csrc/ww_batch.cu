@@ -62,11 +62,10 @@ CfgEntry entry() {
 // Segment bitmaps of 16-128 KB: the whole segment sits in one CTA's shared
 // memory (at most 227 KB per CTA on the B200, so a 256 KB segment cannot be
 // a tile), beside the warps' queues.  128-1024 threads.  1-8 batches of 32
-// PRPs per warp before testing: 4 and 8 only at 256 threads, where they
-// take 78-79 registers without spilling -- at 512 threads (64 registers)
-// they spill 144 and 268 bytes per thread.  The joint test loop (both
-// tests in one loop, 72 registers in the list kernel) at 256 and 512
-// threads.
+// PRPs per warp before testing: 4 and 8 only at 256 threads, with the
+// registers the compiler picks (BatchCfg::kMinBlocks).  The joint test loop
+// (both tests in one loop, 72 registers in the list kernel) at 256 and 512
+// threads, held to 64 registers.
 const std::vector<CfgEntry> &configs() {
     static const std::vector<CfgEntry> table = {
         entry<4096, 128, 1>(),     entry<4096, 256, 1>(),     entry<4096, 512, 1>(),    entry<4096, 256, 2>(),
@@ -86,17 +85,15 @@ const CfgEntry *find_cfg(const ww_batch_cfg &c) {
     return nullptr;
 }
 
-// the configuration the autotuner picks on the uneven mix (64 KB tiles, 512
-// threads, the joint test loop: 835 M primes/s on all 4096 units against
-// 780 M with the tests one after the other)
-ww_batch_cfg default_cfg() { return ww_batch_cfg{16384, 512, 1, 1}; }
+// the configuration the autotuner picks on the uneven mix: 64 KB tiles, 512
+// threads, two CTAs per SM at 64 registers, the tests one after the other
+// (841 M primes/s on its first 128 units, against 774 M for the joint test
+// loop, which needs the same 64 registers with more live state)
+ww_batch_cfg default_cfg() { return ww_batch_cfg{16384, 512, 1, 0}; }
 
 // the request server's unless the caller chose one for the context: the same
-// tile with the tests one after the other.  On 30-s streams at 200 req/s the
-// joint loop gave p50 13.8 ms (p99 69.8 ms) against 7.4 ms (p99 71.4 ms) at
-// the same throughput, twice over; small requests, which finish within a
-// step or two, make the p50.
-ww_batch_cfg default_serve_cfg() { return ww_batch_cfg{16384, 512, 1, 0}; }
+// tile, with one CTA per SM per step (server_init)
+ww_batch_cfg default_serve_cfg() { return default_cfg(); }
 
 }  // namespace
 
@@ -589,7 +586,12 @@ int server_init(ServerState &s, ww_ctx *ctx, const ww_server_cfg *cfg) {
     int per_sm = 0, sms = 0;
     WW_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s.e->serve_kernel, s.e->threads, s.e->smem));
     WW_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx_device(ctx)));
-    s.grid = std::max(1, per_sm) * sms;
+    // a step hands out one tile per CTA, and small requests wait about one
+    // step: with 512 threads' worth of CTAs per SM (one 512-thread tile) the
+    // step is half as long as with the two an SM can hold, for 7 % less
+    // throughput, which the server's load leaves room for
+    const int step_per_sm = std::max(1, std::min(per_sm, 512 / s.e->threads));
+    s.grid = step_per_sm * sms;
     const u32 n = cfg->max_active, h = cfg->max_hits;
     WW_CU(cudaMalloc(&s.d_slots, (size_t)n * sizeof(UnitState)));
     WW_CU(cudaMallocHost(&s.h_slots, (size_t)n * sizeof(UnitState)));

@@ -66,9 +66,15 @@ struct BatchCfg {
     static constexpr int kWarps = THREADS / 32;
     static constexpr int kPpt = PPT;
     static constexpr bool kJoint = JOINT != 0;
-    // joint configurations are held to 1024 threads per SM (64 registers);
-    // the others take what the compiler chooses
-    static constexpr int kMinBlocks = JOINT ? 1024 / THREADS : 1;
+    // resident threads per SM the registers must allow: 1024 (64 registers,
+    // 32 warps) with one or two batches of PRPs per warp -- left to the
+    // compiler, the 512-thread tiles took 128 registers (16 warps per SM)
+    // and ran 7 % slower; four or eight batches keep the compiler's choice
+    // (142 and 146 registers at 256 threads), which measured faster than
+    // 78 and 80 registers at three CTAs per SM (they spill 128 and 256 bytes
+    // at 64)
+    static constexpr int kSmThreads = PPT >= 4 ? THREADS : 1024;
+    static constexpr int kMinBlocks = kSmThreads / THREADS > 0 ? kSmThreads / THREADS : 1;
     static constexpr int kChunks = SEG_WORDS / 32;
     static constexpr u64 kTileNumbers = 64ull * SEG_WORDS;  // integers per tile
     static constexpr int kCandCap = 416;  // as kQueueCap: 31 carried + at most 378 per 32-word chunk

@@ -142,13 +142,15 @@ WW_HD D2 wieferich_digits_t(u64 p, u64 q, D2 one) {
     const int i0 = top_bit(e) - 5;
     const double rp = 1.0 / (double)p;
     D2 a = m2_small(1ull << (u32)(e >> (i0 + 1)), one, p, rp);
+    u64 eb = e << (63 - i0);  // bit i of e at bit 63 in step i
     for (int i = i0; i >= 0; --i) {
         a = ar.sqr(a);
 #if defined(WW_W_WINDOW)
         if (((i0 - i) & 3) == 3) a = m2_mul_pow2(a, (u32)(e >> i) & 15u, p, rp);
 #else
-        a = sel((e >> i) & 1, m2_dbl(a, p), a);
+        a = sel((long long)eb < 0, m2_dbl(a, p), a);
 #endif
+        eb <<= 1;
     }
 #if defined(WW_W_WINDOW)
     const int rest = (i0 + 1) & 3;
@@ -178,9 +180,11 @@ WW_HD D2 wss_digits_t(u64 p, u64 q, D2 one) {
     const double rp = 1.0 / (double)p;
     D2 a = m2_small(lucas_small(k0), one, p, rp);      // V_k0
     D2 b = m2_small(lucas_small(k0 + 1), one, p, rp);  // V_k0+1
-    bool odd = k0 & 1u;  // parity of the ladder index k
+    bool odd = k0 & 1u;      // parity of the ladder index k
+    u64 nb = n << (63 - i0);  // bit i of n at bit 63 in step i
     for (int i = i0; i >= 0; --i) {
-        const bool bit = (n >> i) & 1;
+        const bool bit = (long long)nb < 0;
+        nb <<= 1;
         const D2 c = sel(odd, two, mtwo);  // -2(-1)^k
         const D2 v2k = m2_add(ar.sqr(a), c, p);
         const D2 v2k2 = m2_sub(ar.sqr(b), c, p);
@@ -214,8 +218,14 @@ WW_HD void both_digits_t(u64 p, u64 q, D2 one, D2 &s_out, D2 &c_out) {
     const LadderStart st = ladder_start(p, n, one);
     D2 a = st.a, b = st.b, w = st.w;
     bool odd = st.odd;
+    // bit i of n and of e at bit 63 in step i (shifts by one instead of by i)
+    u64 nb = n << (63 - st.i0);
+    u64 eb = e << (63 - st.i0);
     for (int i = st.i0; i >= 0; --i) {
-        const bool bit = (n >> i) & 1;
+        const bool bit = (long long)nb < 0;
+        const bool ebit = (long long)eb < 0;
+        nb <<= 1;
+        eb <<= 1;
         const D2 a2 = ar.sqr(a);
         const D2 b2 = ar.sqr(b);
         if (i <= st.iw) {
@@ -224,7 +234,7 @@ WW_HD void both_digits_t(u64 p, u64 q, D2 one, D2 &s_out, D2 &c_out) {
             // every fourth bit from iw down: w *= 2^v for the group's four bits
             if (((st.iw - i) & 3) == 3) w = m2_mul_pow2(w, (u32)(e >> i) & 15u, p, st.rp);
 #else
-            w = sel((e >> i) & 1, m2_dbl(w, p), w);
+            w = sel(ebit, m2_dbl(w, p), w);
 #endif
         }
         const D2 c = sel(odd, two, mtwo);     // -2(-1)^k
