@@ -404,6 +404,12 @@ int ww_selftest_range(uint64_t lo, uint64_t hi, uint64_t *prp_count, uint64_t *c
  * Inputs and outputs are digit pairs x0 + p x1; xy = (x0, x1, y0, y1) per
  * case, out = (z0, z1). */
 int ww_selftest_m2(int op, uint64_t p, const uint64_t *xy, uint64_t n, uint64_t *out);
+/* The same check on the device, through the instruction sequences the
+ * kernels run (borrow masks, multiply-pipe corrections): op 0-2 as above,
+ * 3 X+Y, 4 X-Y, 5 2X (mod p^2), and on the low digits alone 6 x0*y0/2^64,
+ * 7 x0+y0, 8 (x1 2^64 + x0)/2^64 (mod p).  Host arrays; synchronises and
+ * allocates its own device copy (no reference counterpart: a test hook). */
+int ww_devtest_m2(int device, int op, uint64_t p, const uint64_t *xy, uint64_t n, uint64_t *out);
 /* The kernels' PRP-test candidates of [lo, hi) computed on the host
  * (small primes 3..113, then the deep sieve, which leaves unmarked every
  * multiple r*k with k = 1 (mod ord_r(2)): r itself and every possible

@@ -18,12 +18,32 @@
 #include <stdint.h>
 
 // On the device the modular corrections (REDC's final subtraction, the
-// two-digit subtraction, the finish of a two-digit product) are written as
-// PTX borrow chains with a mask instead of compare + select; measured 1-2 %
-// faster on the fused test kernel.  -DWW_NO_PTX_CC selects the C forms.
+// two-digit sum and difference, the finish of a two-digit product) are PTX
+// borrow chains: each turns its borrow into a mask m (0 or 2^32 - 1) and
+// adds m & p back, instead of a compare and a select.  -DWW_NO_PTX_CC selects
+// the C forms (measured 3 % slower on the fused test kernel).
 #if !defined(WW_NO_PTX_CC) && !defined(WW_PTX_CC)
 #define WW_PTX_CC 1
 #endif
+//
+// The integer ALU pipe is the busier of the two integer pipes in the test
+// loops (adds, borrows, selects, shifts against the multiplies), so the
+// "& p" of a correction runs as two 32-bit multiplies by the mask on the
+// multiply pipe instead (add_masked, form 2).  WW_MAD_SITES picks where:
+// bit 0 the mod-n REDC and sum of the PRP test, bit 1 the finish of a
+// two-digit product, bit 2 two-digit differences, bit 3 two-digit sums; the
+// places left out keep the ALU form.  Measured on a B200 (fused test kernel,
+// 2^26 primes): sites 1-3 in form 2, 1 318 M primes/s; the ALU mask form
+// everywhere, 1 233 M; the compare/select sums and and+add masks before it,
+// 1 148 M; form 1 (one wide multiply-add) at sites 1-3, 1 117 M.  Bit 0
+// slows the sieve (6.07 against 5.88 ms per 2^30 numbers), so it is off.
+#ifndef WW_MAD_SITES
+#define WW_MAD_SITES 14
+#endif
+#ifndef WW_MAD_FORM
+#define WW_MAD_FORM 2
+#endif
+#define WW_FIX(site) ((WW_MAD_SITES >> (site)) & 1 ? WW_MAD_FORM : 0)
 
 #if defined(__CUDACC__)
 #define WW_HD __host__ __device__ __forceinline__
@@ -55,6 +75,66 @@ WW_HD void mul_wide(u64 a, u64 b, u64 &lo, u64 &hi) {
     hi = mul_hi(a, b);
 }
 
+#if defined(__CUDA_ARCH__) && defined(WW_PTX_CC)
+// r + (m ? p : 0) mod 2^64 for a borrow mask m (0 or 2^32 - 1).
+//   F = 0: r + (p & m:m), an and and an add on the integer ALU;
+//   F = 1: two multiply-adds: with pa = -p_lo and pb = ~p_lo - p_hi (mod 2^32),
+//          m pa + 2^32 (m pb) = p (mod 2^64) for m = 2^32 - 1, since
+//          (2^32 - 1)(pa + 2^32 pb) = 2^32 (pa - pb) - pa = p_lo + 2^32 p_hi;
+//   F = 2: the and as two multiplies (m (-p_lo) = p_lo, m (-p_hi) = p_hi
+//          mod 2^32 for m = 2^32 - 1), then the add with carry.
+// The constants depend on p alone, so loops hoist them.
+template <int F>
+__device__ __forceinline__ u64 add_masked(u64 r, u32 m, u64 p) {
+    u64 t;
+    if (F == 1) {
+        const u32 pa = 0u - (u32)p;
+        const u32 pb = ~(u32)p - (u32)(p >> 32);
+        asm("{\n\t.reg .u32 lo, hi;\n\t"
+            "mad.wide.u32 %0, %1, %2, %3;\n\t"
+            "mov.b64 {lo, hi}, %0;\n\t"
+            "mad.lo.u32 hi, %1, %4, hi;\n\t"
+            "mov.b64 %0, {lo, hi};\n\t}"
+            : "=l"(t) : "r"(m), "r"(pa), "l"(r), "r"(pb));
+    } else if (F == 2) {
+        const u32 pa = 0u - (u32)p;
+        const u32 pc = 0u - (u32)(p >> 32);
+        asm("{\n\t.reg .u32 a0, a1, r0, r1;\n\t"
+            "mul.lo.u32 a0, %1, %2;\n\t"
+            "mul.lo.u32 a1, %1, %3;\n\t"
+            "mov.b64 {r0, r1}, %4;\n\t"
+            "add.cc.u32 r0, r0, a0;\n\t"
+            "addc.u32 r1, r1, a1;\n\t"
+            "mov.b64 %0, {r0, r1};\n\t}"
+            : "=l"(t) : "r"(m), "r"(pa), "r"(pc), "l"(r));
+    } else {
+        asm("{\n\t.reg .u64 mm;\n\t"
+            "mov.b64 mm, {%1, %1};\n\t"
+            "and.b64 mm, mm, %2;\n\t"
+            "add.u64 %0, %3, mm;\n\t}"
+            : "=l"(t) : "r"(m), "l"(p), "l"(r));
+    }
+    return t;
+}
+
+// a + b - n mod 2^64 for a + b < 2n, and in m the sign of the exact value:
+// (c:s) = a + b, then m = c - borrow of s - n (0, or -1 when a + b < n).
+// Flags set by an add are read by adds and flags set by a subtraction by
+// subtractions only: ptxas does not carry the PTX meaning of the flag from
+// an add.cc into a subc (measured on sm_100a: after an add.cc without carry,
+// subc subtracted one).
+__device__ __forceinline__ u64 sum_minus(u64 a, u64 b, u64 n, u32 &m) {
+    u64 t;
+    asm("{\n\t.reg .u32 c;\n\t"
+        "add.cc.u64 %0, %2, %3;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "sub.cc.u64 %0, %0, %4;\n\t"
+        "subc.u32 %1, c, 0;\n\t}"
+        : "=&l"(t), "=r"(m) : "l"(a), "l"(b), "l"(n));
+    return t;
+}
+#endif
+
 // n^-1 mod 2^64 (Newton; n*n = 1 mod 8 seeds 3 correct bits).
 WW_HD u64 inv64(u64 n) {
     u64 x = n;
@@ -69,8 +149,14 @@ WW_HD u64 inv64(u64 n) {
 // ------------------------------------------------------------------- mod n
 
 WW_HD u64 add_mod(u64 a, u64 b, u64 n) {  // a <= n, b < n
+#if defined(__CUDA_ARCH__) && defined(WW_PTX_CC) && (WW_MAD_SITES & 1)
+    u32 m;
+    const u64 t = sum_minus(a, b, n, m);
+    return add_masked<WW_FIX(0)>(t, m, n);
+#else
     u64 s = a + b;
     return (s < a || s >= n) ? s - n : s;
+#endif
 }
 
 WW_HD u64 sub_mod(u64 a, u64 b, u64 n) {  // a < n, b <= n
@@ -81,7 +167,14 @@ WW_HD u64 sub_mod(u64 a, u64 b, u64 n) {  // a < n, b <= n
 WW_HD u64 redc(u64 lo, u64 hi, u64 n, u64 q) {
     u64 u = lo * q;
     u64 v = mul_hi(u, n);
-#if defined(__CUDA_ARCH__) && defined(WW_PTX_CC)
+#if defined(__CUDA_ARCH__) && defined(WW_PTX_CC) && (WW_MAD_SITES & 1)
+    u64 r;
+    u32 m;
+    asm("sub.cc.u64 %0, %2, %3;\n\t"  // hi - v, borrow-out
+        "subc.u32 %1, 0, 0;"          // -borrow
+        : "=&l"(r), "=r"(m) : "l"(hi), "l"(v));
+    return add_masked<WW_FIX(0)>(r, m, n);
+#elif defined(__CUDA_ARCH__) && defined(WW_PTX_CC)
     u64 r;
     asm("{\n\t.reg .u64 m;\n\t"
         "sub.cc.u64 %0, %1, %2;\n\t"  // hi - v, borrow-out
@@ -268,18 +361,42 @@ struct ModP2 {
 
 WW_HD D2 m2_add(D2 x, D2 y, u64 p) {
     D2 r;
+#if defined(__CUDA_ARCH__) && defined(WW_PTX_CC) && (WW_MAD_SITES & 8)
+    // low digit: (c:s) = x0 + y0 - p with m0 = c - borrow (0 or -1); the
+    // high digit x1 + (1 + m0) + y1 - p the same way (x1 + 1 + m0 <= p)
+    u32 m0, m1;
+    const u64 t0 = sum_minus(x.d0, y.d0, p, m0);
+    const u64 t1 = sum_minus(x.d1 + (u64)(m0 + 1u), y.d1, p, m1);
+    r.d0 = add_masked<WW_FIX(3)>(t0, m0, p);
+    r.d1 = add_masked<WW_FIX(3)>(t1, m1, p);
+#else
     u64 s = x.d0 + y.d0;
     bool c = (s < x.d0) | (s >= p);
     r.d0 = c ? s - p : s;
     u64 h = x.d1 + (u64)c;  // <= p
     u64 t = h + y.d1;
     r.d1 = ((t < h) | (t >= p)) ? t - p : t;
+#endif
     return r;
 }
 
 WW_HD D2 m2_sub(D2 x, D2 y, u64 p) {
     D2 r;
-#if defined(__CUDA_ARCH__) && defined(WW_PTX_CC)
+#if defined(__CUDA_ARCH__) && defined(WW_PTX_CC) && (WW_MAD_SITES & 4)
+    // one borrow chain through both digits; each digit's borrow-out becomes a
+    // mask (subc without .cc leaves the flag for the next digit)
+    u64 t0, t1;
+    u32 m0, m1;
+    asm("sub.cc.u64 %0, %4, %6;\n\t"
+        "subc.u32 %2, 0, 0;\n\t"
+        "subc.cc.u64 %1, %5, %7;\n\t"  // x1 - y1 - borrow
+        "subc.u32 %3, 0, 0;"
+        : "=&l"(t0), "=&l"(t1), "=&r"(m0), "=&r"(m1)
+        : "l"(x.d0), "l"(x.d1), "l"(y.d0), "l"(y.d1));
+    r.d0 = add_masked<WW_FIX(2)>(t0, m0, p);
+    r.d1 = add_masked<WW_FIX(2)>(t1, m1, p);
+    return r;
+#elif defined(__CUDA_ARCH__) && defined(WW_PTX_CC)
     // one borrow chain through both digits; each digit adds p back on its
     // own borrow-out
     asm("{\n\t.reg .u64 m0, m1;\n\t"
@@ -312,7 +429,39 @@ WW_HD D2 m2_finish(u64 alo, u64 ahi, u64 clo, u64 chi, u64 ctop, u64 p, u64 q) {
     const u64 u = alo * q;
     const u64 v = mul_hi(u, p);
     D2 r;
-#if defined(__CUDA_ARCH__) && defined(WW_PTX_CC)
+#if defined(__CUDA_ARCH__) && defined(WW_PTX_CC) && (WW_MAD_SITES & 2)
+    u64 t0, s, t1, t2;
+    u32 mb, mh, md;
+    // low digit ahi - v, plus p on borrow (mb = -borrow)
+    asm("sub.cc.u64 %0, %2, %3;\n\t"
+        "subc.u32 %1, 0, 0;"
+        : "=&l"(t0), "=r"(mb) : "l"(ahi), "l"(v));
+    r.d0 = add_masked<WW_FIX(1)>(t0, mb, p);
+    // (k:h) = (C + u) >> 64 < 2p and s its low word; then (k:h) - p with
+    // mh = k - borrow, which is -1 exactly when (k:h) < p
+    asm("{\n\t.reg .u32 k;\n\t.reg .u64 h;\n\t"
+        "add.cc.u64 %0, %3, %4;\n\t"
+        "addc.cc.u64 h, %5, 0;\n\t"
+        "addc.u32 k, %6, 0;\n\t"
+        "sub.cc.u64 %1, h, %7;\n\t"
+        "subc.u32 %2, k, 0;\n\t}"
+        : "=&l"(s), "=&l"(t1), "=&r"(mh)
+        : "l"(clo), "l"(u), "l"(chi), "r"((u32)ctop), "l"(p));
+    const u64 h2 = add_masked<WW_FIX(1)>(t1, mh, p);
+    const u64 v2 = mul_hi(s * q, p);
+    // high digit h2 - v2 - borrow of the low digit (the flag set again from
+    // mb: 0 - mb borrows exactly when mb = -1), plus p on borrow.  Every flag
+    // here is set by a subtraction and read by one: ptxas does not carry the
+    // PTX meaning of the flag from an add.cc into a subc (measured on sm_100a:
+    // after an add.cc without carry, subc subtracted one).
+    asm("{\n\t.reg .u32 z;\n\t"
+        "sub.cc.u32 z, 0, %2;\n\t"
+        "subc.cc.u64 %0, %3, %4;\n\t"
+        "subc.u32 %1, 0, 0;\n\t}"
+        : "=&l"(t2), "=r"(md) : "r"(mb), "l"(h2), "l"(v2));
+    r.d1 = add_masked<WW_FIX(1)>(t2, md, p);
+    return r;
+#elif defined(__CUDA_ARCH__) && defined(WW_PTX_CC)
     u64 mb, s, h, k, h2;
     // low digit ahi - v, plus p on borrow; mb = -borrow
     asm("{\n\t.reg .u64 t;\n\t"

@@ -159,6 +159,34 @@ WW_HD D2 wieferich_digits_t(u64 p, u64 q, D2 one) {
     return ar.redc(a);
 }
 
+// One step of the Lucas ladder kept as (e, o): for the pair of indices
+// (k, k+1), e is V at the even one and o is V at the odd one up to sign.
+// Since V_2m = V_m^2 - 2(-1)^m, x = e^2 - 2 and y = o^2 + 2 are V at twice
+// the even and twice the odd index, whatever the parity of k, and their
+// difference is V_2k+1 up to sign (y - x = +V_2k+1 for k even, -V_2k+1 for k
+// odd), which the next squaring does not see.  The new pair is (2k, 2k+1)
+// for bit 0 and (2k+1, 2k+2) for bit 1; its even index is 2k or 2k+2, so e
+// becomes x or y by the bit and the parity of k.  Against a ladder on
+// (V_k, V_k+1) this saves the selection of the constant -2(-1)^k and one of
+// the two pair selections.  two and mtwo: 2 and -2 in Montgomery form.
+template <class A>
+WW_HD void eo_step(const A &ar, D2 &e, D2 &o, bool &kodd, bool bit, D2 two, D2 mtwo, u64 p) {
+    const D2 x = m2_sub(ar.sqr(e), two, p);   // V_2k (k even) or V_2k+2 (k odd)
+    const D2 y = m2_sub(ar.sqr(o), mtwo, p);  // the other of the two
+    o = m2_sub(y, x, p);
+    e = sel(bit != kodd, y, x);
+    kodd = bit;
+}
+
+// 2 V_n+1 - V_n for the ladder's final (e, o) at k = n, n even (n = p +- 1):
+// e = V_n, and o = y - x of the last step, from k = n/2, is +V_n+1 when n/2
+// is even (bit 1 of n clear) and -V_n+1 when it is odd.
+WW_HD D2 eo_finish(D2 e, D2 o, u64 n, u64 p) {
+    const D2 zero = {0, 0};
+    const D2 t = m2_dbl(o, p);
+    return m2_sub(((n >> 1) & 1) ? m2_sub(zero, t, p) : t, e, p);
+}
+
 // F_{p-(p|5)} mod p^2 as canonical digits.  The reference walks the
 // (F_k, F_{k-1}) doubling ladder, two squarings and a product per bit
 // (wallsunsun.cl:242-300).  Here the Lucas numbers V_k = L_k run a ladder
@@ -178,22 +206,33 @@ WW_HD D2 wss_digits_t(u64 p, u64 q, D2 one) {
     const int i0 = top_bit(n) - 6;
     const u32 k0 = (u32)(n >> (i0 + 1));
     const double rp = 1.0 / (double)p;
-    D2 a = m2_small(lucas_small(k0), one, p, rp);      // V_k0
-    D2 b = m2_small(lucas_small(k0 + 1), one, p, rp);  // V_k0+1
+    const D2 a = m2_small(lucas_small(k0), one, p, rp);      // V_k0
+    const D2 b = m2_small(lucas_small(k0 + 1), one, p, rp);  // V_k0+1
     bool odd = k0 & 1u;      // parity of the ladder index k
     u64 nb = n << (63 - i0);  // bit i of n at bit 63 in step i
+#if !defined(WW_NO_EO_LADDER)
+    D2 e = sel(odd, b, a), o = sel(odd, a, b);
+    for (int i = i0; i >= 0; --i) {
+        const bool bit = (long long)nb < 0;
+        nb <<= 1;
+        eo_step(ar, e, o, odd, bit, two, mtwo, p);
+    }
+    const D2 t = ar.redc(eo_finish(e, o, n, p));
+#else
+    D2 va = a, vb = b;
     for (int i = i0; i >= 0; --i) {
         const bool bit = (long long)nb < 0;
         nb <<= 1;
         const D2 c = sel(odd, two, mtwo);  // -2(-1)^k
-        const D2 v2k = m2_add(ar.sqr(a), c, p);
-        const D2 v2k2 = m2_sub(ar.sqr(b), c, p);
+        const D2 v2k = m2_add(ar.sqr(va), c, p);
+        const D2 v2k2 = m2_sub(ar.sqr(vb), c, p);
         const D2 v2k1 = m2_sub(v2k2, v2k, p);
-        a = sel(bit, v2k1, v2k);
-        b = sel(bit, v2k2, v2k1);
+        va = sel(bit, v2k1, v2k);
+        vb = sel(bit, v2k2, v2k1);
         odd = bit;
     }
-    const D2 t = ar.redc(m2_sub(m2_dbl(b, p), a, p));
+    const D2 t = ar.redc(m2_sub(m2_dbl(vb, p), va, p));
+#endif
     return m2_div5(t, p);
 }
 
@@ -216,11 +255,36 @@ WW_HD void both_digits_t(u64 p, u64 q, D2 one, D2 &s_out, D2 &c_out) {
     const D2 two = m2_dbl(one, p);
     const D2 mtwo = m2_sub(zero, two, p);
     const LadderStart st = ladder_start(p, n, one);
-    D2 a = st.a, b = st.b, w = st.w;
+    D2 w = st.w;
     bool odd = st.odd;
     // bit i of n and of e at bit 63 in step i (shifts by one instead of by i)
     u64 nb = n << (63 - st.i0);
     u64 eb = e << (63 - st.i0);
+#if !defined(WW_NO_EO_LADDER)
+    D2 le = sel(odd, st.b, st.a), lo = sel(odd, st.a, st.b);
+    for (int i = st.i0; i >= 0; --i) {
+        const bool bit = (long long)nb < 0;
+        const bool ebit = (long long)eb < 0;
+        nb <<= 1;
+        eb <<= 1;
+        eo_step(ar, le, lo, odd, bit, two, mtwo, p);
+        if (i <= st.iw) {
+            w = ar.sqr(w);
+#if defined(WW_W_WINDOW)
+            if (((st.iw - i) & 3) == 3) w = m2_mul_pow2(w, (u32)(e >> i) & 15u, p, st.rp);
+#else
+            w = sel(ebit, m2_dbl(w, p), w);
+#endif
+        }
+    }
+#if defined(WW_W_WINDOW)
+    const int rest = (st.iw + 1) & 3;
+    if (rest) w = m2_mul_pow2(w, (u32)e & ((1u << rest) - 1u), p, st.rp);
+#endif
+    s_out = ar.redc(w);
+    c_out = m2_div5(ar.redc(eo_finish(le, lo, n, p)), p);
+#else
+    D2 a = st.a, b = st.b;
     for (int i = st.i0; i >= 0; --i) {
         const bool bit = (long long)nb < 0;
         const bool ebit = (long long)eb < 0;
@@ -251,6 +315,7 @@ WW_HD void both_digits_t(u64 p, u64 q, D2 one, D2 &s_out, D2 &c_out) {
 #endif
     s_out = ar.redc(w);
     c_out = m2_div5(ar.redc(m2_sub(m2_dbl(b, p), a, p)), p);
+#endif
 }
 
 WW_HD D2 wieferich_digits(u64 p, u64 q, D2 one) { return wieferich_digits_t<WW_ARITH>(p, q, one); }

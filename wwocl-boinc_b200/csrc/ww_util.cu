@@ -10,6 +10,7 @@
 
 #include "../../include/wwcuda.h"
 #include "ww_arith.cuh"
+#include "ww_tests.cuh"
 
 using namespace ww;
 
@@ -141,6 +142,33 @@ __global__ void k_pipe(int iters, u32 seed, u32 *sink) {
     if (acc == 0x7fffffffu) sink[threadIdx.x] = acc;  // keeps the chains live
 }
 
+// One operation of the device arithmetic per case (the instruction sequences
+// the kernels run), for checking it operand by operand: ops 0-2 as
+// ww_selftest_m2, 3 X+Y, 4 X-Y, 5 2X (mod p^2), 6 x0*y0/2^64, 7 x0+y0,
+// 8 (x1:x0)/2^64 (mod p).
+__global__ void k_m2_cases(int op, u64 p, const u64 *xy, u64 n, u64 *out) {
+    const u64 q = inv64(p);
+    const WW_ARITH ar(p, q);
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const D2 x = {xy[4 * i], xy[4 * i + 1]};
+        const D2 y = {xy[4 * i + 2], xy[4 * i + 3]};
+        D2 z = {0, 0};
+        switch (op) {
+            case 0: z = ar.mul(x, y); break;
+            case 1: z = ar.sqr(x); break;
+            case 2: z = ar.redc(x); break;
+            case 3: z = m2_add(x, y, p); break;
+            case 4: z = m2_sub(x, y, p); break;
+            case 5: z = m2_dbl(x, p); break;
+            case 6: z.d0 = mont_mul(x.d0, y.d0, p, q); break;
+            case 7: z.d0 = add_mod(x.d0, y.d0, p); break;
+            default: z.d0 = redc(x.d0, x.d1, p, q); break;
+        }
+        out[2 * i] = z.d0;
+        out[2 * i + 1] = z.d1;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -177,6 +205,25 @@ int ww_random_primes(int device, uint64_t seed, uint64_t n, uint64_t *out, uint6
     }
     cudaFree(dbits);
     if (consumed) *consumed = used;
+    return rc;
+}
+
+int ww_devtest_m2(int device, int op, uint64_t p, const uint64_t *xy, uint64_t n, uint64_t *out) {
+    if ((p & 1) == 0 || p < 3 || ((!xy || !out) && n) || op < 0 || op > 8) return WW_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return WW_ERR_NODEV;
+    if (n == 0) return WW_OK;
+    u64 *d = nullptr;
+    if (cudaMalloc(&d, n * 48) != cudaSuccess) return WW_ERR_NOMEM;
+    int rc = WW_OK;
+    if (cudaMemcpy(d, xy, n * 32, cudaMemcpyHostToDevice) != cudaSuccess) rc = WW_ERR_CUDA;
+    if (rc == WW_OK) {
+        const u64 blocks = (n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184;
+        k_m2_cases<<<(unsigned)blocks, 256>>>(op, p, d, n, d + 4 * n);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpy(out, d + 4 * n, n * 16, cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = WW_ERR_CUDA;
+    }
+    cudaFree(d);
     return rc;
 }
 

@@ -163,6 +163,7 @@ _SIGS = {
     "ww_server_prps": (C.c_int, [_VP, C.c_uint64, _VP, C.c_uint64, C.POINTER(C.c_uint64)]),
     "ww_batch_run_noalloc": (C.c_int, [C.POINTER(Unit), C.c_uint32, _VP, _VP, _VP, C.c_uint32, _VP, _VP]),
     "ww_selftest_m2": (C.c_int, [C.c_int, C.c_uint64, _U64P, C.c_uint64, _U64P]),
+    "ww_devtest_m2": (C.c_int, [C.c_int, C.c_int, C.c_uint64, _U64P, C.c_uint64, _U64P]),
     "ww_selftest_candidates": (C.c_int, [C.c_uint64, C.c_uint64, _U64P, C.c_uint64, C.POINTER(C.c_uint64),
                                          C.POINTER(C.c_uint64)]),
     "ww_random_primes": (C.c_int, [C.c_int, C.c_uint64, C.c_uint64, _U64P, C.POINTER(C.c_uint64)]),
@@ -259,6 +260,14 @@ def selftest_m2(op: int, p: int, xy: np.ndarray) -> np.ndarray:
     n = xy.size // 4
     out = np.zeros(2 * n, dtype=np.uint64)
     check(_L.ww_selftest_m2(op, p, xy, n, out), "ww_selftest_m2")
+    return out.reshape(-1, 2)
+
+
+def devtest_m2(op: int, p: int, xy: np.ndarray, device: int = 0) -> np.ndarray:
+    xy = np.ascontiguousarray(xy, dtype=np.uint64).reshape(-1)
+    n = xy.size // 4
+    out = np.zeros(2 * n, dtype=np.uint64)
+    check(_L.ww_devtest_m2(device, op, p, xy, n, out), "ww_devtest_m2")
     return out.reshape(-1, 2)
 
 
