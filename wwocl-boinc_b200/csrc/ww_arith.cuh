@@ -33,10 +33,13 @@
 // bit 0 the mod-n REDC and sum of the PRP test, bit 1 the finish of a
 // two-digit product, bit 2 two-digit differences, bit 3 two-digit sums; the
 // places left out keep the ALU form.  Measured on a B200 (fused test kernel,
-// 2^26 primes): sites 1-3 in form 2, 1 318 M primes/s; the ALU mask form
-// everywhere, 1 233 M; the compare/select sums and and+add masks before it,
-// 1 148 M; form 1 (one wide multiply-add) at sites 1-3, 1 117 M.  Bit 0
-// slows the sieve (6.07 against 5.88 ms per 2^30 numbers), so it is off.
+// 2^26 primes, before the three-product square): sites 1-3 in form 2,
+// 1 318 M primes/s; sites 1-2, 1 340 M (with the square); sites 1 and 3 or
+// 2 and 3, 1 283 and 1 216 M; the ALU mask form everywhere, 1 233 M; the
+// compare/select sums and and+add masks before it, 1 148 M; form 1 (one wide
+// multiply-add) at sites 1-3, 1 117 M; mad.lo.cc/madc.lo (the add fused into
+// the multiply with a carry), 1 279 M against 1 364 M.  Bit 0 slows the sieve
+// (6.07 against 5.88 ms per 2^30 numbers), so it is off.
 #ifndef WW_MAD_SITES
 #define WW_MAD_SITES 14
 #endif
@@ -73,6 +76,20 @@ WW_HD u64 mul_hi(u64 a, u64 b) {
 WW_HD void mul_wide(u64 a, u64 b, u64 &lo, u64 &hi) {
     lo = a * b;
     hi = mul_hi(a, b);
+}
+
+// a^2 as (hi:lo) from three 32x32 products (a0^2, a1^2 and a0 a1 once):
+// a^2 = a0^2 + 2^33 a0 a1 + 2^64 a1^2.  Used for the low digit of a
+// two-digit square, where it measured 3.5 % faster on the fused test kernel
+// than the four-product mul_wide; in the PRP test's squaring and as the
+// high word of a REDC's u*p (three products, with the carry of the known
+// low word) it measured slower.
+WW_HD void sqr_wide(u64 a, u64 &lo, u64 &hi) {
+    const u32 a0 = (u32)a, a1 = (u32)(a >> 32);
+    const u64 m = (u64)a0 * a1;
+    const u64 t = m << 33;
+    lo = (u64)a0 * a0 + t;
+    hi = (u64)a1 * a1 + (m >> 31) + (u64)(lo < t);
 }
 
 #if defined(__CUDA_ARCH__) && defined(WW_PTX_CC)
@@ -193,6 +210,7 @@ WW_HD u64 mont_mul(u64 a, u64 b, u64 n, u64 q) {
     mul_wide(a, b, lo, hi);
     return redc(lo, hi, n, q);
 }
+
 
 // For odd n in [2^32, 2^63): q = floor(2^64 / n) and 2^64 - q n.  On the
 // device the quotient comes from a double-precision estimate (off by at most
@@ -527,7 +545,7 @@ WW_HD D2 m2_mul(D2 x, D2 y, u64 p, u64 q) {
 
 WW_HD D2 m2_sqr(D2 x, u64 p, u64 q) {
     u64 alo, ahi, l, h;
-    mul_wide(x.d0, x.d0, alo, ahi);
+    sqr_wide(x.d0, alo, ahi);
     mul_wide(x.d0, x.d1, l, h);
     const u64 ctop = h >> 63;
     const u64 chi = (h << 1) | (l >> 63);
