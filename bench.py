@@ -86,7 +86,9 @@ def config(args, world):
 def algorithmic_imad_per_prime(primes: np.ndarray) -> tuple[float, float]:
     """32-bit multiply instructions per prime, counted with fixed costs: a
     64x64->128 product = 8, a low 64-bit product = 4, a high 64-bit product =
-    8, so a two-digit square mod p^2 = 40 and a product = 48.  k = bitlength(p).
+    8, so a two-digit square mod p^2 = 40 and a product = 48 (38 for the
+    square k_test_prps runs, whose low digit is squared from three 32x32
+    products instead of four).  k = bitlength(p).
 
     Returns (reference_count, executed_count):
       reference_count: the reference kernels' algorithm -- Wieferich k-3
@@ -95,11 +97,11 @@ def algorithmic_imad_per_prime(primes: np.ndarray) -> tuple[float, float]:
       executed_count: what k_test_prps runs -- both ladders start from the
         top bits of their exponents (three small numbers turned into
         Montgomery form, 40 each), then Wieferich k-6 squarings and the Lucas
-        ladder k-6 steps of two squarings, two conversions out of Montgomery
-        form (24 each): 120(k-6) + 120 + 48."""
+        ladder k-6 steps of two squarings (38 each), two conversions out of
+        Montgomery form (24 each): 114(k-6) + 120 + 48."""
     bits = np.floor(np.log2(primes.astype(np.float64))) + 1  # exact away from powers of two
     ref = 40.0 * (bits - 3) + 128.0 * (bits - 1)
-    run = 120.0 * (bits - 6) + 168.0
+    run = 114.0 * (bits - 6) + 168.0
     return float(ref.mean()), float(run.mean())
 
 
@@ -270,7 +272,7 @@ def run_range_pipeline(ww, local: int, width: int, ckpt: int = 1 << 30, chain_pe
         k = 64
         ref_ops = 40.0 * (k - 3) + 128.0 * (k - 1) + 5.3 * 20.0 * (k - 1)
         cand = (0.5615 / np.log(2.0**depth)) * np.log(2.0**64)
-        run_ops = 120.0 * (k - 6) + 168.0 + cand * (20.0 * (k - 5) + 12.0)
+        run_ops = 114.0 * (k - 6) + 168.0 + cand * (20.0 * (k - 5) + 12.0)
         rate = out["primes_per_s"]
         out["roofline_end_to_end"] = {
             "peak_tops": chain_peak / 1e12,
@@ -645,7 +647,7 @@ def main():
                 "ops_source": "reference kernels' algorithm: 40(k-3) + 128(k-1) 32-bit multiplies per prime",
                 "executed": {"ops_per_prime": per_prime_run, "achieved": achieved_run / 1e12,
                              "frac": achieved_run / chain_peak,
-                             "note": "multiplies k_test_prps itself runs: 120(k-6) + 168 (ladders started from their top bits)"},
+                             "note": "multiplies k_test_prps itself runs: 114(k-6) + 168 (ladders started from their top bits, three-product squares of the low digit)"},
                 "mad_lo_only": {"peak": madlo_peak / 1e12, "frac": achieved / madlo_peak,
                                 "frac_executed": achieved_run / madlo_peak},
                 "hbm": {"bytes_per_launch": 16 * n, "GBps": 16 * n / (launch_ms * 1e-3) / 1e9,
