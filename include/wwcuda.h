@@ -284,8 +284,9 @@ int ww_batch_tune(ww_ctx *ctx, const ww_unit *sample, uint32_t n, ww_batch_cfg *
  * NULL) and *hit_count are device memory; work is queued on `stream` (a
  * cudaStream_t) and the call does not wait for it.  Calls share the array:
  * each clears it, and calls whose GPU work overlaps race, so keep them on
- * one stream.  The first call on a device also looks up the array's address
- * (cudaGetSymbolAddress) once.  *hit_count receives the number of hits found.  When that exceeds
+ * one stream.  The first call on a device does a one-time set-up (it looks
+ * up the array's address with cudaGetSymbolAddress); make that first call
+ * before any stream capture.  *hit_count receives the number of hits found.  When that exceeds
  * min(hit_cap, 4096), the records hold that many of them, in no set
  * order, and out[i].hits still counts every hit of range i.
  * Returns WW_ERR_ARG for more than 4096 ranges. */

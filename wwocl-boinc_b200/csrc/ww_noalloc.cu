@@ -19,7 +19,8 @@
 // different host threads) race on it -- order them on one stream.  The
 // first call on each device does a one-time set-up (the device addresses of
 // the array and of the library's deep-sieve table, and the kernel's
-// shared-memory attribute).
+// shared-memory attribute); that first call should come before any stream
+// capture.
 #include <cuda_runtime.h>
 
 #include <cstring>
