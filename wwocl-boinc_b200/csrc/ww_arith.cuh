@@ -38,8 +38,9 @@
 // 2 and 3, 1 283 and 1 216 M; the ALU mask form everywhere, 1 233 M; the
 // compare/select sums and and+add masks before it, 1 148 M; form 1 (one wide
 // multiply-add) at sites 1-3, 1 117 M; mad.lo.cc/madc.lo (the add fused into
-// the multiply with a carry), 1 279 M against 1 364 M.  Bit 0 slows the sieve
-// (6.07 against 5.88 ms per 2^30 numbers), so it is off.
+// the multiply with a carry), 1 279 M against 1 364 M; the same two
+// multiplies written in C, 1 221 M, or as asm on 32-bit halves, 1 349 M.
+// Bit 0 slows the sieve (6.07 against 5.88 ms per 2^30 numbers), so it is off.
 #ifndef WW_MAD_SITES
 #define WW_MAD_SITES 14
 #endif
