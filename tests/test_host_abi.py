@@ -380,3 +380,15 @@ def test_host_twin_range_at_boundaries(ww, oracle, lo, hi):
     assert got["prp_count"] == want["prp_count"]
     assert got["checksum"] == want["checksum"]
     assert got["result_count"] == want["gpu_results"]
+
+
+def test_devtest_m2_rejects_bad_arguments(ww):
+    """The device arithmetic check refuses an even or too small modulus and an
+    unknown operation before it touches a device, and does nothing for zero
+    cases."""
+    xy = np.zeros(4, dtype=np.uint64)
+    for op, p in [(0, 2**64 - 2), (0, 1), (9, 2**64 - 59), (-1, 2**64 - 59)]:
+        with pytest.raises(ww.WWError) as e:
+            ww.devtest_m2(op, p, xy)
+        assert e.value.status == -2
+    assert ww.devtest_m2(1, 2**64 - 59, np.zeros(0, dtype=np.uint64)).shape == (0, 2)

@@ -210,8 +210,8 @@ int ww_random_primes(int device, uint64_t seed, uint64_t n, uint64_t *out, uint6
 
 int ww_devtest_m2(int device, int op, uint64_t p, const uint64_t *xy, uint64_t n, uint64_t *out) {
     if ((p & 1) == 0 || p < 3 || ((!xy || !out) && n) || op < 0 || op > 8) return WW_ERR_ARG;
-    if (cudaSetDevice(device) != cudaSuccess) return WW_ERR_NODEV;
     if (n == 0) return WW_OK;
+    if (cudaSetDevice(device) != cudaSuccess) return WW_ERR_NODEV;
     u64 *d = nullptr;
     if (cudaMalloc(&d, n * 48) != cudaSuccess) return WW_ERR_NOMEM;
     int rc = WW_OK;
