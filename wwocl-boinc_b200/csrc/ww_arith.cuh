@@ -26,10 +26,11 @@
 #define WW_PTX_CC 1
 #endif
 //
-// The integer ALU pipe is the busier of the two integer pipes in the test
-// loops (adds, borrows, selects, shifts against the multiplies), so the
-// "& p" of a correction runs as two 32-bit multiplies by the mask on the
-// multiply pipe instead (add_masked, form 2).  WW_MAD_SITES picks where:
+// With every correction on the integer ALU, that pipe was the busier of the
+// two integer pipes in the test loops (73 % against 71 %: adds, borrows,
+// selects and shifts outnumber the multiplies), so the "& p" of a correction
+// runs as two 32-bit multiplies by the mask on the multiply pipe instead
+// (add_masked, form 2), which leaves the multiply pipe the busier one.  WW_MAD_SITES picks where:
 // bit 0 the mod-n REDC and sum of the PRP test, bit 1 the finish of a
 // two-digit product, bit 2 two-digit differences, bit 3 two-digit sums; the
 // places left out keep the ALU form.  Measured on a B200 (fused test kernel,
