@@ -22,6 +22,14 @@
 
 namespace ww {
 
+// Threads per SM the sieve's launch bounds ask for: 1024 holds it to 64
+// registers (2 CTAs of 512, or 4 of 256, per SM).  Uncapped it takes 128;
+// at 512 or 768 (1 CTA of 512 per SM, 128 registers) the sieve measured
+// 7.19 against 5.90 ms per 2^30 numbers on a B200.
+#ifndef WW_SIEVE_MINB_THREADS
+#define WW_SIEVE_MINB_THREADS 1024
+#endif
+
 // Sieve + SPRP over [lo, hi) in segments of shape G (SieveGeom).  b0 = lo & ~1;
 // segment s holds the odd numbers b0 + 2(s*G::kOdd + j) + 1, j < G::kOdd.
 // With a segment cursor (zeroed before the launch) the CTAs take segments
@@ -31,7 +39,7 @@ namespace ww {
 // launch, bit j of word w = odd number b0 + 2(32 w + j) + 1 (ww_bucket.cu),
 // ORed into each segment's bitmap.
 template <class G>
-__global__ void __launch_bounds__(G::kThreads, 1024 / G::kThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out,
+__global__ void __launch_bounds__(G::kThreads, WW_SIEVE_MINB_THREADS / G::kThreads) k_sieve_prp(u64 lo, u64 hi, u64 nseg, PrpOut out,
                                                                               u64 *cursor, const DeepRow *deep,
                                                                               const u32 *__restrict__ marks) {
     extern __shared__ u32 sieve_smem[];  // G::kSmem bytes
