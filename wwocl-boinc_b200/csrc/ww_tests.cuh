@@ -194,7 +194,9 @@ WW_HD D2 eo_finish(D2 e, D2 o, u64 n, u64 p) {
 //   V_2k = V_k^2 - 2(-1)^k,  V_2k+2 = V_k+1^2 + 2(-1)^k,  V_2k+1 = V_2k+2 - V_2k,
 // and F_n = (2 V_{n+1} - V_n) / 5 gives the same residue exactly (5 is a
 // unit mod p^2 since p has no factor below 127).  The ladder starts from
-// the top six bits of n (ladder_start).
+// the top six bits of n (ladder_start) and keeps its pair as (V at the even
+// index, V at the odd index up to sign), eo_step; -DWW_NO_EO_LADDER keeps
+// (V_k, V_k+1) instead.
 template <class A>
 WW_HD D2 wss_digits_t(u64 p, u64 q, D2 one) {
     const A ar(p, q);
@@ -244,7 +246,7 @@ WW_HD D2 wss_digits_t(u64 p, u64 q, D2 one) {
 // so the three products of an iteration are squarings, independent of each
 // other, and no operand has to be selected before multiplying.  Both start
 // from their top bits (ladder_start), the Wieferich powering at most one
-// bit after the ladder.
+// bit after the ladder; the Lucas pair is kept as eo_step's (e, o).
 template <class A>
 WW_HD void both_digits_t(u64 p, u64 q, D2 one, D2 &s_out, D2 &c_out) {
     const A ar(p, q);
